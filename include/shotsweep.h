@@ -1,0 +1,152 @@
+/*
+ * shotsweep.h - C ABI of libshotsweep, the sm_100a (B200) implementation of
+ * ShotSweep's physics hot path: the batched 2-D constant-density acoustic
+ * finite-difference simulator and its exact discrete adjoint, which produce
+ * surface gathers, per-shot velocity gradients, source illumination and
+ * reverse-time-migration (RTM) images.
+ *
+ * The reference is pure Python (openfwi/physics/gpu.py); it has no FFI.  Each
+ * entry point below replaces the computational core of one method of the
+ * reference's `Sim` class or one module-level helper, and is what a ctypes
+ * binding of that method calls (see INTEGRATION.md for the binding).
+ *
+ * Conventions
+ *   - All array pointers are DEVICE pointers, C-contiguous float32 unless the
+ *     name says f64.  Outputs are caller-allocated.
+ *   - Every compute call is asynchronous and ordered on `stream` (a
+ *     cudaStream_t passed as void*; NULL = legacy default stream).
+ *   - Return value: SS_OK (0) or a negative ss_status; the message of the last
+ *     failure on the calling thread is available from ss_last_error().
+ *   - The simulation entry points need a device workspace of
+ *     ss_workspace_bytes(...) bytes.  Device-side failures (a bounded wait that
+ *     ran out) are recorded in the workspace; ss_workspace_status() reads them
+ *     back after synchronising `stream`.
+ *   - Per-solve geometry follows the reference: padded grid
+ *     (nz+2*pad) x (nx+2*pad), sources and receivers on model row `src_row`,
+ *     receivers at every model column, wavelet samples already scaled by the
+ *     caller (the reference multiplies by 1e3, gpu.py:94).
+ */
+#ifndef SHOTSWEEP_H
+#define SHOTSWEEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SS_MAX_SHOTS 16
+
+typedef enum ss_status {
+    SS_OK = 0,
+    SS_ERR_INVALID = -1,      /* bad argument (shape, pointer, range)          */
+    SS_ERR_UNSUPPORTED = -2,  /* geometry does not fit any kernel plan         */
+    SS_ERR_CUDA = -3,         /* a CUDA runtime call failed                    */
+    SS_ERR_TIMEOUT = -4,      /* a device-side bounded wait ran out            */
+    SS_ERR_WORKSPACE = -5,    /* workspace missing or smaller than required    */
+    SS_ERR_NONFINITE = -6     /* observed gathers hold NaN or infinity         */
+} ss_status;
+
+/* Acquisition and grid of one batch (reference: openfwi/physics/constants.py:4-7,
+ * Sim.__init__ gpu.py:77-96).  Defaults of the reference: nz=nx=70, nt=1000,
+ * pad=40, n_shots=5, shot_cols={0,17,34,52,69}, src_row=1, dx=10, dt=1e-3,
+ * r_coef=1e-5, vmax_damping=4500, amp_ref=2000. */
+typedef struct ss_geometry {
+    int32_t nz, nx;                     /* model cells (rows, columns)                    */
+    int32_t nt;                         /* time steps                                     */
+    int32_t pad;                        /* absorbing-layer width in cells (>= 2)          */
+    int32_t n_shots;                    /* shots per velocity model (1..SS_MAX_SHOTS)     */
+    int32_t src_row;                    /* model row of sources and receivers             */
+    int32_t shot_cols[SS_MAX_SHOTS];    /* source columns in model coordinates            */
+    double dx, dt;                      /* grid spacing (m) and time step (s)             */
+    double r_coef;                      /* target reflection coefficient R of the layer   */
+    double vmax_damping;                /* velocity in the damping constant (4500)        */
+    double amp_ref;                     /* source-strength normalisation velocity (2000)  */
+} ss_geometry;
+
+typedef enum ss_mode {
+    SS_MODE_FORWARD = 0,   /* gathers only                         */
+    SS_MODE_GRADIENT = 1,  /* forward + adjoint -> gradient, illum  */
+    SS_MODE_IMAGES = 2     /* gradient + image epilogue             */
+} ss_mode;
+
+/* Library version string. */
+const char* ss_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* ss_last_error(void);
+
+/* Bytes of device workspace that a call with this geometry, number of
+ * velocity models and mode needs on the current device. */
+size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mode);
+
+/* Reads the device-side status word of `workspace` after synchronising
+ * `stream`: SS_OK, SS_ERR_TIMEOUT if a bounded wait ran out, or
+ * SS_ERR_NONFINITE if the observed gathers held a non-finite sample (the
+ * reference rejects those with ValueError, gpu.py:156-157; outputs of such a
+ * call are undefined). */
+int32_t ss_workspace_status(const void* workspace, void* stream);
+
+/* Kernel plan for diagnostics: out[0..7] = cluster size (CTAs per solve),
+ * threads per CTA, dynamic shared bytes per CTA, band rows per CTA, column
+ * groups, rows per thread, co-resident clusters on this device, solves
+ * in flight for n_models. */
+int32_t ss_plan_info(const ss_geometry* geom, int32_t n_models, int32_t mode, int64_t out[8]);
+
+/* Forward modelling.  Replaces Sim.forward / Sim.gathers (gpu.py:117-140).
+ *   vel      [n_models, nz, nx]                    velocities (m/s)
+ *   wavelet  [nt]                                  scaled source samples
+ *   gathers  [n_models, n_shots, nt, nx]           output: receiver traces
+ *   ckpt     NULL or [n_models, n_shots, ceil(nt/ckpt_interval), 2, nz+2pad, nx+2pad]
+ *            output: wavefields (p0, p1) before every ckpt_interval-th step,
+ *            as Sim.forward(store=True) keeps them (gpu.py:130-132); the
+ *            caller zero-fills it (its 2-cell border is never written). */
+int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                   float* gathers, float* ckpt, int32_t ckpt_interval,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Per-shot gradient of 0.5*sum(w*(sim-obs)^2) and source illumination.
+ * Replaces Sim._gradient / Sim.gradient (gpu.py:152-194).
+ *   obs      [n_models, n_shots, nt, nx]   observed gathers
+ *   v_mute   NULL (no mute) or [n_models]   mute velocities (gpu.py:142-150)
+ *   grad     [n_models, n_shots, nz, nx]    output
+ *   illum    [n_models, n_shots, nz, nx]    output: sum over steps of Laplacian^2 */
+int32_t ss_gradient(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                    const float* obs, const float* v_mute, float t_mute,
+                    float* grad, float* illum,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* RTM images: illumination-normalised negative gradients, optionally
+ * Laplacian filtered.  Replaces Sim.images (gpu.py:196-210).
+ *   img      [n_models, n_shots, nz, nx]    output
+ *   illum    [n_models, n_shots, nz, nx]    output
+ *   grad     NULL or [n_models, n_shots, nz, nx]  optional output */
+int32_t ss_images(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                  const float* obs, const float* v_mute, float t_mute, float eps, int32_t laplacian,
+                  float* img, float* illum, float* grad,
+                  void* workspace, size_t workspace_bytes, void* stream);
+
+/* Module helpers (gpu.py:33-67, 142-150, 105-107) on device arrays whose last
+ * two axes are (n0, n1); `batch` is the product of the leading axes. */
+int32_t ss_lap_f32(const float* p, float* out, int64_t batch, int32_t n0, int32_t n1, void* stream);
+int32_t ss_lap_f64(const double* p, double* out, int64_t batch, int32_t n0, int32_t n1, void* stream);
+int32_t ss_lap_adjoint_f32(const float* p, float* out, int64_t batch, int32_t n0, int32_t n1, void* stream);
+int32_t ss_lap_adjoint_f64(const double* p, double* out, int64_t batch, int32_t n0, int32_t n1, void* stream);
+/* g [batch, nz+2pad, nx+2pad] -> out [batch, nz, nx] (transpose of edge padding). */
+int32_t ss_fold_edge_padding_f32(const float* g, float* out, int64_t batch, int32_t nz, int32_t nx,
+                                 int32_t pad, void* stream);
+int32_t ss_fold_edge_padding_f64(const double* g, double* out, int64_t batch, int32_t nz, int32_t nx,
+                                 int32_t pad, void* stream);
+/* Direct-wave mute weights [n_models, n_shots, nt, nx] (gpu.py:142-150). */
+int32_t ss_mute_weights(const ss_geometry* geom, int32_t n_models, const float* v_mute, float t_mute,
+                        float* out, void* stream);
+/* Squared Courant numbers of the edge-padded model, c2 = v^2 (dt/dx)^2,
+ * [n_models, nz+2pad, nx+2pad] (gpu.py:105-107). */
+int32_t ss_c2_field(const ss_geometry* geom, int32_t n_models, const float* vel, float* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHOTSWEEP_H */

@@ -1,0 +1,1105 @@
+// libshotsweep: B200 (sm_100a) kernels for ShotSweep's physics hot path.
+//
+// One velocity model x one shot is a "solve".  Each solve runs on a thread-block
+// cluster of C CTAs (C = 2 for the 150x150 padded OpenFWI grid); the padded grid
+// is cut into C horizontal bands, one per CTA, and each CTA keeps its band of
+// the two most recent wavefields in shared memory for the whole time loop.
+// Neighbouring bands exchange their two edge rows every step through
+// distributed shared memory (DSMEM); one cluster barrier per step orders it.
+//
+// Arithmetic (reference: openfwi/physics/gpu.py)
+//   forward   p[t+1] = p[t-1] + kappa*(p[t]-p[t-1]) + sigma*S(p[t])  (+ source)
+//   adjoint   th[t]  = th[t+2] + kappa*(th[t+1]-th[t+2]) + sigma*S(th[t+1]) (+ sigma*res)
+// with S the 9-point 4th-order Laplacian times 12*dx^2, kappa = 2A and
+// sigma = c2*A/12 masked to the interior (zero on the 2-cell border).  The
+// forward is the reference update (2p1 - B p0 + c2 L) A (gpu.py:111-115)
+// rewritten with A*B = 2A - 1 (true for A = 1/(1+a), B = 1-a).  The adjoint is
+// the reference adjoint mu = 2A m1 + lap^T(c2 A m1) - A B m2 (gpu.py:179)
+// after the diagonal change of variable th = sigma*mu, which gives it the same
+// form as the forward; the gradient becomes g*2v(dt/dx)^2 = 2/v * sum_t th*S(p)
+// and mu at the source is th/sigma there (gpu.py:181-187).
+//
+// Instead of the reference's checkpoint-and-recompute (gpu.py:131,169-176) the
+// forward stores S(p[t]) of every step to a per-cluster history in HBM with
+// TMA bulk copies (cp.async.bulk) and the adjoint streams it back in reverse,
+// prefetching one step ahead.  This trades 2x4 bytes of HBM traffic per cell
+// and step for the 16 flops per cell and step that a recompute would cost.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/shotsweep.h"
+
+namespace {
+
+constexpr int kRowsPerThread = 6;          // H: rows per thread in the band
+constexpr int kMaxThreads = 512;           // register budget: 128 regs/thread
+constexpr int kMaxCluster = 16;
+constexpr size_t kMaxSmem = 227 * 1024;
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s per bounded wait
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define SS_CUDA(call)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(SS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+// ----------------------------------------------------------------------------
+// PTX helpers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_id() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster_v4(uint32_t addr, float4 v) {
+  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w)
+               : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after kWaitLimitNs, records SS_ERR_TIMEOUT and
+// returns, so that every thread still reaches every barrier of the kernel.
+__device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity, int* err) {
+  if (mbar_try_wait(bar, parity)) return;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > kWaitLimitNs) {
+      atomicExch(err, static_cast<int>(SS_ERR_TIMEOUT));
+      return;
+    }
+  }
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_all() { asm volatile("fence.proxy.async;" ::: "memory"); }
+
+// 9-point stencil times 12*dx^2: 16*(near) - (far) - 60*centre.
+__device__ __forceinline__ float stencil(float zm2, float zm1, float c, float zp1, float zp2, float xm2, float xm1,
+                                         float xp1, float xp2) {
+  const float near_ = (zm1 + zp1) + (xm1 + xp1);
+  const float far_ = (zm2 + zp2) + (xm2 + xp2);
+  return fmaf(-60.f, c, fmaf(16.f, near_, -far_));
+}
+
+// Normalised depth into the absorbing layer (gpu.py:85-87).
+__device__ __forceinline__ double layer_depth(int i, int n, int pad) {
+  const int d = max(max(pad - i, i - (n - 1 - pad)), 0);
+  return static_cast<double>(d) / pad;
+}
+
+// ----------------------------------------------------------------------------
+// Fused per-solve kernel
+// ----------------------------------------------------------------------------
+struct KParams {
+  int nz, nx, nt, pad, nzp, nxp, n_shots, src_row;
+  int shot_cols[SS_MAX_SHOTS];
+  double dtdx2, damp_k, amp_ref;
+  float dx, dt;
+  int ncg, nseg, bh, C, rs, sw, nact;
+  int nxs;         // trace row stride of the per-slot scratch (nx rounded up to 4)
+  int n_solves;
+  const float* vel;
+  const float* wav;
+  const float* obs;
+  const float* vmute;
+  float t_mute;
+  float* gathers;  // forward mode output [solve][nt][nx]
+  float* trace;    // per-slot scratch [nt][nx]
+  float* illum;
+  float* grad;     // output, or per-slot scratch [nz][nx]
+  int grad_per_slot;
+  float* img;
+  float* gpad;     // per-slot scratch [nzp][nxp]
+  float* hist;     // per-slot [nt][C][bh*sw]
+  float* ckpt;
+  int ckpt_interval, n_ckpt;
+  float eps;
+  int laplacian;
+  int* err;
+};
+
+struct Smem {
+  float* f[2];
+  float* stg[2];
+  float* wav;
+  float* red;
+  float* res[2];   // residual row of the current / next adjoint step
+  uint64_t* bar;
+};
+
+__device__ __forceinline__ float mute_weight(int t, int r, int shot_col, float dx, float dt, float vm, float t_mute) {
+  // gpu.py:146-150 in float32: h/v_mute + t_mute, 30 ms cosine ramp.
+  const float h = fabsf(static_cast<float>(r) * dx - static_cast<float>(shot_col) * dx);
+  const float tt = static_cast<float>(t) * dt;
+  const float t0 = h / vm + t_mute;
+  const float ramp = fminf(fmaxf((tt - t0) / 0.03f, 0.f), 1.f);
+  return 0.5f - 0.5f * cosf(3.14159265358979323846f * ramp);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) {
+  constexpr int H = kRowsPerThread;
+  constexpr bool ADJ = MODE != SS_MODE_FORWARD;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int rank = static_cast<int>(cluster_rank());
+  const int slot = static_cast<int>(cluster_id());
+  const int n_slots = static_cast<int>(cluster_count());
+
+  // ---- shared-memory carve-up (identical in every CTA of the cluster) ----
+  Smem S;
+  {
+    const size_t field = static_cast<size_t>(P.bh + 4) * P.rs;
+    const size_t stage = ADJ ? static_cast<size_t>(P.bh) * P.sw : 0;
+    float* base = reinterpret_cast<float*>(smem_raw);
+    S.f[0] = base;
+    S.f[1] = base + field;
+    S.stg[0] = base + 2 * field;
+    S.stg[1] = base + 2 * field + stage;
+    S.wav = base + 2 * field + 2 * stage;
+    S.red = S.wav + ((P.nt + 31) & ~31);
+    S.res[0] = S.red + 32;
+    S.res[1] = S.res[0] + P.nxs;
+    S.bar = reinterpret_cast<uint64_t*>(S.res[1] + P.nxs);
+  }
+  for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
+  if (ADJ && tid == 0) {
+    mbar_init(smem_u32(&S.bar[0]), 1);
+    mbar_init(smem_u32(&S.bar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  uint32_t phase_bits = 0;   // parity of the next wait on each staging buffer
+
+  // ---- this thread's block of cells: H rows x 4 columns -----------------
+  const bool active = tid < P.nact;
+  const int cg = active ? tid % P.ncg : 0;
+  const int seg = active ? tid / P.ncg : 0;
+  const int row0 = 2 + rank * P.bh;               // first padded row of the band
+  const int myrow = row0 + seg * H;               // first padded row of this thread
+  const int col0 = 2 + 4 * cg;                    // first padded column
+  const int o0 = 4 * cg + 4;                      // shared-memory column offset of col0
+  const int lr0 = seg * H;                        // shared row of window row k=-2
+  const int src_r = P.pad + P.src_row;            // padded row of sources and receivers
+  const int rec_rank = (src_r - 2) / P.bh;
+
+  // Halo pushes to the neighbouring bands (rows needed by their stencils).
+  const bool push_up = active && seg == 0 && rank > 0;
+  const bool push_dn = active && seg == P.nseg - 1 && rank < P.C - 1;
+  // Remote addresses in buffer 0; buffer 1 lies field_bytes further on.
+  const uint32_t field_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh + 4) * P.rs * sizeof(float));
+  const uint32_t up_addr = push_up ? mapa(smem_u32(S.f[0] + (P.bh + 2) * P.rs + o0), rank - 1) : 0u;
+  const uint32_t dn_addr = push_dn ? mapa(smem_u32(S.f[0] + o0), rank + 1) : 0u;
+
+  const int rec_k = (active && src_r >= myrow && src_r < myrow + H) ? src_r - myrow : -1;
+
+  const size_t field_floats = static_cast<size_t>(P.bh + 4) * P.rs;
+  const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * P.sw * sizeof(float));
+  const size_t hist_slot = static_cast<size_t>(P.nt) * P.C * P.bh * P.sw;
+  float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * P.sw
+                               : nullptr;
+  const size_t hist_step = static_cast<size_t>(P.C) * P.bh * P.sw;
+
+  cluster_sync();   // barriers initialised and wavelet staged everywhere
+
+  for (int solve = slot; solve < P.n_solves; solve += n_slots) {
+    const int b = solve / P.n_shots;
+    const int s = solve - b * P.n_shots;
+    const float* v = P.vel + static_cast<size_t>(b) * P.nz * P.nx;
+    const int shot_col = P.shot_cols[s];
+    const int src_c = P.pad + shot_col;
+
+    // ---- per-cell coefficients ----------------------------------------
+    float kap[H][4], sig[H][4], acc[H][4];
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int r = myrow + k, c = col0 + m;
+        kap[k][m] = 0.f;
+        sig[k][m] = 0.f;
+        acc[k][m] = 0.f;
+        if (active && r < P.nzp - 2 && c < P.nxp - 2) {
+          const double dz = layer_depth(r, P.nzp, P.pad), dxl = layer_depth(c, P.nxp, P.pad);
+          const float A = static_cast<float>(1.0 / (1.0 + P.damp_k * (dz * dz + dxl * dxl)));
+          const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
+          const double vp = v[vz * P.nx + vx];
+          const float c2 = static_cast<float>(vp * vp * P.dtdx2);
+          kap[k][m] = 2.f * A;
+          sig[k][m] = (c2 * A) / 12.f;
+        }
+      }
+    }
+    int src_k = -1, src_m = 0;
+    if (active && src_r >= myrow && src_r < myrow + H && src_c >= col0 && src_c < col0 + 4) {
+      src_k = src_r - myrow;
+      src_m = src_c - col0;
+    }
+    const double v_src = v[P.src_row * P.nx + shot_col];
+    const float amp = static_cast<float>((v_src / P.amp_ref) * (v_src / P.amp_ref));
+
+    const int tstride = (MODE == SS_MODE_FORWARD) ? P.nx : P.nxs;
+    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + static_cast<size_t>(solve) * P.nt * P.nx
+                                             : P.trace + static_cast<size_t>(slot) * P.nt * P.nxs;
+
+    // ---- zero both wavefields (own rows and halos) ---------------------
+    for (size_t i = tid; i < field_floats / 2; i += nthr) {
+      reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
+      reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
+    }
+    cluster_sync();
+
+    // ================= forward: t = 0 .. nt-1 =============================
+    int cur = 0;   // S.f[cur] = p[t], S.f[cur^1] = p[t-1]
+    for (int t = 0; t < P.nt; ++t) {
+      const float* X = cur ? S.f[1] : S.f[0];
+      float* Y = cur ? S.f[0] : S.f[1];
+      if (MODE == SS_MODE_FORWARD && P.ckpt != nullptr && t % P.ckpt_interval == 0 && active) {
+        float* ck = P.ckpt + ((static_cast<size_t>(solve) * P.n_ckpt + t / P.ckpt_interval) * 2) * P.nzp * P.nxp;
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+          const int r = myrow + k;
+          if (r >= P.nzp - 2) break;
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const int c = col0 + m;
+            if (c < P.nxp - 2) {
+              ck[static_cast<size_t>(r) * P.nxp + c] = Y[(lr0 + k + 2) * P.rs + o0 + m];
+              ck[static_cast<size_t>(P.nzp) * P.nxp + static_cast<size_t>(r) * P.nxp + c] =
+                  X[(lr0 + k + 2) * P.rs + o0 + m];
+            }
+          }
+        }
+      }
+      if (active) {
+        const float wt = S.wav[t] * amp;
+        const float* xc = X + lr0 * P.rs + o0;
+        float4 r0 = *reinterpret_cast<const float4*>(xc);
+        float4 r1 = *reinterpret_cast<const float4*>(xc + P.rs);
+        float4 r2 = *reinterpret_cast<const float4*>(xc + 2 * P.rs);
+        float4 r3 = *reinterpret_cast<const float4*>(xc + 3 * P.rs);
+        float* stg = ADJ ? ((t & 1) ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg : nullptr;
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+          const float4 r4 = *reinterpret_cast<const float4*>(xc + (k + 4) * P.rs);
+          const float* rowc = xc + (k + 2) * P.rs;
+          const float2 lf = *reinterpret_cast<const float2*>(rowc - 2);
+          const float2 rt = *reinterpret_cast<const float2*>(rowc + 4);
+          float4 L;
+          L.x = stencil(r0.x, r1.x, r2.x, r3.x, r4.x, lf.x, lf.y, r2.y, r2.z);
+          L.y = stencil(r0.y, r1.y, r2.y, r3.y, r4.y, lf.y, r2.x, r2.z, r2.w);
+          L.z = stencil(r0.z, r1.z, r2.z, r3.z, r4.z, r2.x, r2.y, r2.w, rt.x);
+          L.w = stencil(r0.w, r1.w, r2.w, r3.w, r4.w, r2.y, r2.z, rt.x, rt.y);
+          float* yp = Y + (lr0 + k + 2) * P.rs + o0;
+          const float4 p0 = *reinterpret_cast<const float4*>(yp);
+          float4 p2;
+          p2.x = fmaf(sig[k][0], L.x, fmaf(kap[k][0], r2.x - p0.x, p0.x));
+          p2.y = fmaf(sig[k][1], L.y, fmaf(kap[k][1], r2.y - p0.y, p0.y));
+          p2.z = fmaf(sig[k][2], L.z, fmaf(kap[k][2], r2.z - p0.z, p0.z));
+          p2.w = fmaf(sig[k][3], L.w, fmaf(kap[k][3], r2.w - p0.w, p0.w));
+          if (k == src_k) {   // injection after damping (gpu.py:113-114)
+            if (src_m == 0) p2.x += wt;
+            else if (src_m == 1) p2.y += wt;
+            else if (src_m == 2) p2.z += wt;
+            else p2.w += wt;
+          }
+          *reinterpret_cast<float4*>(yp) = p2;
+          if (push_up && k < 2) st_cluster_v4(up_addr + (cur ^ 1) * field_bytes + 4u * (k * P.rs), p2);
+          if (push_dn && k >= H - 2)
+            st_cluster_v4(dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * P.rs), p2);
+          if (ADJ) {
+            *reinterpret_cast<float4*>(stg + k * P.sw) = L;
+            acc[k][0] = fmaf(L.x, L.x, acc[k][0]);
+            acc[k][1] = fmaf(L.y, L.y, acc[k][1]);
+            acc[k][2] = fmaf(L.z, L.z, acc[k][2]);
+            acc[k][3] = fmaf(L.w, L.w, acc[k][3]);
+          }
+          if (k == rec_k) {   // receivers at every model column (gpu.py:134)
+            float* tr = trace + static_cast<size_t>(t) * tstride + (col0 - P.pad);
+            const int rr = col0 - P.pad;
+            if (rr >= 0 && rr < P.nx) tr[0] = p2.x;
+            if (rr + 1 >= 0 && rr + 1 < P.nx) tr[1] = p2.y;
+            if (rr + 2 >= 0 && rr + 2 < P.nx) tr[2] = p2.z;
+            if (rr + 3 >= 0 && rr + 3 < P.nx) tr[3] = p2.w;
+          }
+          r0 = r1;
+          r1 = r2;
+          r2 = r3;
+          r3 = r4;
+        }
+      }
+      if (ADJ) {
+        fence_proxy_async_smem();
+        if (tid == 0 && t > 0) bulk_wait_read_all();   // store of step t-1 has left shared memory
+      }
+      cluster_sync();
+      if (ADJ && tid == 0)
+        bulk_store(hist_mine + static_cast<size_t>(t) * hist_step, smem_u32((t & 1) ? S.stg[1] : S.stg[0]), stage_bytes);
+      cur ^= 1;
+    }
+
+    if (MODE == SS_MODE_FORWARD) continue;
+
+    // ---- forward epilogue: illumination = sum_t (S/12)^2 on model cells --
+    if (tid == 0) {
+      bulk_wait_all();
+      fence_proxy_async_all();
+    }
+    {
+      float* il = P.illum + static_cast<size_t>(solve) * P.nz * P.nx;
+#pragma unroll
+      for (int k = 0; k < H; ++k)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int z = myrow + k - P.pad, x = col0 + m - P.pad;
+          if (active && z >= 0 && z < P.nz && x >= 0 && x < P.nx)
+            il[z * P.nx + x] = acc[k][m] * (1.f / 144.f);
+          acc[k][m] = 0.f;
+        }
+    }
+    // ---- residual (sim - obs) * mute, in place over the trace ------------
+    if (rank == rec_rank) {
+      const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * P.nx;
+      const float vm = P.vmute ? P.vmute[b] : 0.f;
+      for (int i = tid; i < P.nt * P.nx; i += nthr) {
+        const int t = i / P.nx, r = i - t * P.nx;
+        const float o = ob[i];
+        if (!isfinite(o)) atomicExch(P.err, static_cast<int>(SS_ERR_NONFINITE));
+        float res = trace[t * P.nxs + r] - o;
+        if (P.vmute) res *= mute_weight(t, r, shot_col, P.dx, P.dt, vm, P.t_mute);
+        trace[t * P.nxs + r] = res;
+      }
+      fence_proxy_async_all();   // these rows are read back by bulk copies
+      __syncthreads();
+    }
+
+    // ================= adjoint: t = nt-1 .. 0 =============================
+    for (size_t i = tid; i < field_floats / 2; i += nthr) {
+      reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
+      reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
+    }
+    float src_acc = 0.f;
+    const bool res_here = rank == rec_rank;
+    const uint32_t res_bytes = static_cast<uint32_t>(P.nxs * sizeof(float));
+    // One bulk copy brings the history slab of step t, one more (on the band
+    // with the receivers) the residual row of step t; both signal bar[t&1].
+    auto issue = [&](int t) {
+      const int bi = t & 1;
+      const uint32_t bar = smem_u32(&S.bar[0]) + 8u * bi;
+      mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
+      bulk_load(smem_u32(bi ? S.stg[1] : S.stg[0]), hist_mine + static_cast<size_t>(t) * hist_step, stage_bytes, bar);
+      if (res_here) bulk_load(smem_u32(bi ? S.res[1] : S.res[0]), trace + static_cast<size_t>(t) * P.nxs, res_bytes, bar);
+    };
+    cluster_sync();
+    if (tid == 0) issue(P.nt - 1);
+    cur = 0;   // S.f[cur] = th[t+1], S.f[cur^1] = th[t+2]
+    for (int t = P.nt - 1; t >= 0; --t) {
+      const float* X = cur ? S.f[1] : S.f[0];
+      float* Y = cur ? S.f[0] : S.f[1];
+      if (tid == 0 && t > 0) issue(t - 1);
+      const int bi = t & 1;
+      mbar_wait_bounded(smem_u32(&S.bar[0]) + 8u * bi, (phase_bits >> bi) & 1u, P.err);
+      phase_bits ^= 1u << bi;
+      if (active) {
+        const float wt = S.wav[t];
+        const float* xc = X + lr0 * P.rs + o0;
+        const float* hl = (bi ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg;
+        float4 r0 = *reinterpret_cast<const float4*>(xc);
+        float4 r1 = *reinterpret_cast<const float4*>(xc + P.rs);
+        float4 r2 = *reinterpret_cast<const float4*>(xc + 2 * P.rs);
+        float4 r3 = *reinterpret_cast<const float4*>(xc + 3 * P.rs);
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+          const float4 r4 = *reinterpret_cast<const float4*>(xc + (k + 4) * P.rs);
+          const float* rowc = xc + (k + 2) * P.rs;
+          const float2 lf = *reinterpret_cast<const float2*>(rowc - 2);
+          const float2 rt = *reinterpret_cast<const float2*>(rowc + 4);
+          float4 L;
+          L.x = stencil(r0.x, r1.x, r2.x, r3.x, r4.x, lf.x, lf.y, r2.y, r2.z);
+          L.y = stencil(r0.y, r1.y, r2.y, r3.y, r4.y, lf.y, r2.x, r2.z, r2.w);
+          L.z = stencil(r0.z, r1.z, r2.z, r3.z, r4.z, r2.x, r2.y, r2.w, rt.x);
+          L.w = stencil(r0.w, r1.w, r2.w, r3.w, r4.w, r2.y, r2.z, rt.x, rt.y);
+          float* yp = Y + (lr0 + k + 2) * P.rs + o0;
+          const float4 q2 = *reinterpret_cast<const float4*>(yp);
+          float4 q;
+          q.x = fmaf(sig[k][0], L.x, fmaf(kap[k][0], r2.x - q2.x, q2.x));
+          q.y = fmaf(sig[k][1], L.y, fmaf(kap[k][1], r2.y - q2.y, q2.y));
+          q.z = fmaf(sig[k][2], L.z, fmaf(kap[k][2], r2.z - q2.z, q2.z));
+          q.w = fmaf(sig[k][3], L.w, fmaf(kap[k][3], r2.w - q2.w, q2.w));
+          if (k == rec_k) {   // residual injection on the receiver row (gpu.py:180)
+            const float* rs = bi ? S.res[1] : S.res[0];
+            const int rr = col0 - P.pad;
+            if (rr >= 0 && rr < P.nx) q.x = fmaf(sig[k][0], rs[rr], q.x);
+            if (rr + 1 >= 0 && rr + 1 < P.nx) q.y = fmaf(sig[k][1], rs[rr + 1], q.y);
+            if (rr + 2 >= 0 && rr + 2 < P.nx) q.z = fmaf(sig[k][2], rs[rr + 2], q.z);
+            if (rr + 3 >= 0 && rr + 3 < P.nx) q.w = fmaf(sig[k][3], rs[rr + 3], q.w);
+          }
+          *reinterpret_cast<float4*>(yp) = q;
+          if (push_up && k < 2) st_cluster_v4(up_addr + (cur ^ 1) * field_bytes + 4u * (k * P.rs), q);
+          if (push_dn && k >= H - 2)
+            st_cluster_v4(dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * P.rs), q);
+          const float4 h = *reinterpret_cast<const float4*>(hl + k * P.sw);
+          acc[k][0] = fmaf(q.x, h.x, acc[k][0]);
+          acc[k][1] = fmaf(q.y, h.y, acc[k][1]);
+          acc[k][2] = fmaf(q.z, h.z, acc[k][2]);
+          acc[k][3] = fmaf(q.w, h.w, acc[k][3]);
+          if (k == src_k) {   // source-strength derivative (gpu.py:182)
+            const float qs = src_m == 0 ? q.x : src_m == 1 ? q.y : src_m == 2 ? q.z : q.w;
+            src_acc = fmaf(qs, wt, src_acc);
+          }
+          r0 = r1;
+          r1 = r2;
+          r2 = r3;
+          r3 = r4;
+        }
+      }
+      cluster_sync();
+      cur ^= 1;
+    }
+
+    // ---- padded gradient 2/v * sum_t th*S(p), plus the source term -------
+    float* gp = P.gpad + static_cast<size_t>(slot) * P.nzp * P.nxp;
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < H; ++k)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int r = myrow + k, c = col0 + m;
+          if (r < P.nzp - 2 && c < P.nxp - 2) {
+            const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
+            const float vp = v[vz * P.nx + vx];
+            float gval = 2.f * acc[k][m] / vp;
+            if (k == src_k && m == src_m) {
+              const float deriv = static_cast<float>(2.0 * v_src / (P.amp_ref * P.amp_ref));
+              gval += src_acc * deriv / sig[k][m];
+            }
+            gp[static_cast<size_t>(r) * P.nxp + c] = gval;
+          }
+        }
+    }
+    __threadfence();
+    cluster_sync();
+
+    // ---- fold the padding onto the edge cells (gpu.py:56-67, 185-187) ----
+    float* go = P.grad_per_slot ? P.grad + static_cast<size_t>(slot) * P.nz * P.nx
+                                : P.grad + static_cast<size_t>(solve) * P.nz * P.nx;
+    {
+      const int zlo = 2, zhi = P.nzp - 2, xlo = 2, xhi = P.nxp - 2;
+      auto G = [&](int i, int j) -> float { return gp[static_cast<size_t>(i) * P.nxp + j]; };
+      const int gthr = rank * nthr + tid, gstride = P.C * nthr;
+      for (int o = gthr; o < P.nz * P.nx; o += gstride) {
+        const int z = o / P.nx, x = o - z * P.nx;
+        const bool zc = (z == 0 || z == P.nz - 1), xc = (x == 0 || x == P.nx - 1);
+        if (zc && xc) continue;   // corners: one warp each below
+        const int i = P.pad + z, j = P.pad + x;
+        float val = G(i, j);
+        if (z == 0)
+          for (int ii = zlo; ii < P.pad; ++ii) val += G(ii, j);
+        if (z == P.nz - 1)
+          for (int ii = P.pad + P.nz; ii < zhi; ++ii) val += G(ii, j);
+        if (x == 0)
+          for (int jj = xlo; jj < P.pad; ++jj) val += G(i, jj);
+        if (x == P.nx - 1)
+          for (int jj = P.pad + P.nx; jj < xhi; ++jj) val += G(i, jj);
+        go[o] = val;
+      }
+      const int warp = tid >> 5, lane = tid & 31;
+      if (rank == 0 && warp < 4) {
+        const int z = (warp & 1) ? P.nz - 1 : 0, x = (warp & 2) ? P.nx - 1 : 0;
+        const int i = P.pad + z, j = P.pad + x;
+        const int i0 = z == 0 ? zlo : P.pad + P.nz, i1 = z == 0 ? P.pad : zhi;
+        const int j0 = x == 0 ? xlo : P.pad + P.nx, j1 = x == 0 ? P.pad : xhi;
+        float val = 0.f;
+        for (int ii = i0 + lane; ii < i1; ii += 32) val += G(ii, j);   // strip above/below
+        for (int jj = j0 + lane; jj < j1; jj += 32) val += G(i, jj);   // strip left/right
+        const int bw = j1 - j0, bn = (i1 - i0) * bw;
+        for (int q = lane; q < bn; q += 32) val += G(i0 + q / bw, j0 + q % bw);   // corner block
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) val += __shfl_xor_sync(0xffffffffu, val, off);
+        if (lane == 0) go[z * P.nx + x] = G(i, j) + val;
+      }
+    }
+    if (MODE == SS_MODE_IMAGES) {
+      __threadfence();
+      cluster_sync();
+      // ---- image epilogue (gpu.py:206-209) --------------------------------
+      const float* il = P.illum + static_cast<size_t>(solve) * P.nz * P.nx;
+      float mx = -INFINITY;
+      for (int o = tid; o < P.nz * P.nx; o += nthr) mx = fmaxf(mx, il[o]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if ((tid & 31) == 0) S.red[tid >> 5] = mx;
+      __syncthreads();
+      if (tid < 32) {
+        float w = tid < (nthr + 31) / 32 ? S.red[tid] : -INFINITY;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) w = fmaxf(w, __shfl_xor_sync(0xffffffffu, w, off));
+        if (tid == 0) S.red[0] = w;
+      }
+      __syncthreads();
+      const float emax = P.eps * S.red[0];
+      float* pre = gp;   // reuse the padded-gradient scratch for the unfiltered image
+      const int gthr = rank * nthr + tid, gstride = P.C * nthr;
+      for (int o = gthr; o < P.nz * P.nx; o += gstride) {
+        const float den = fmaxf(il[o] + emax, 1.17549435e-38f);
+        pre[o] = -go[o] / den;
+      }
+      float* im = P.img + static_cast<size_t>(solve) * P.nz * P.nx;
+      if (P.laplacian) {
+        __threadfence();
+        cluster_sync();
+        for (int o = gthr; o < P.nz * P.nx; o += gstride) {
+          const int z = o / P.nx, x = o - z * P.nx;
+          auto I = [&](int zz, int xx) -> float {
+            zz = min(max(zz, 0), P.nz - 1);
+            xx = min(max(xx, 0), P.nx - 1);
+            return pre[zz * P.nx + xx];
+          };
+          const float c = I(z, x);
+          const float lz = -I(z - 2, x) + 16.f * I(z - 1, x) - 30.f * c + 16.f * I(z + 1, x) - I(z + 2, x);
+          const float lx = -I(z, x - 2) + 16.f * I(z, x - 1) - 30.f * c + 16.f * I(z, x + 1) - I(z, x + 2);
+          im[o] = -((lz + lx) / 12.f);
+        }
+      } else {
+        for (int o = gthr; o < P.nz * P.nx; o += gstride) im[o] = pre[o];
+      }
+    }
+    __threadfence();
+    cluster_sync();   // scratch of this slot is free for the next solve
+  }
+  cluster_sync();     // no CTA leaves while a neighbour may still write its shared memory
+}
+
+// ----------------------------------------------------------------------------
+// Small helper kernels (module-level functions of the reference)
+// ----------------------------------------------------------------------------
+template <typename T>
+__global__ void lap_kernel(const T* __restrict__ p, T* __restrict__ out, long long batch, int n0, int n1) {
+  const long long total = batch * n0 * n1;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(idx % n1);
+    const int i = static_cast<int>((idx / n1) % n0);
+    T val = T(0);
+    if (i >= 2 && i < n0 - 2 && j >= 2 && j < n1 - 2) {
+      const T* q = p + idx;
+      const T c = q[0];
+      const T z = -q[-2 * n1] + T(16) * q[-n1] - T(30) * c + T(16) * q[n1] - q[2 * n1];
+      const T x = -q[-2] + T(16) * q[-1] - T(30) * c + T(16) * q[1] - q[2];
+      val = (z + x) / T(12);
+    }
+    out[idx] = val;
+  }
+}
+
+template <typename T>
+__global__ void lap_adjoint_kernel(const T* __restrict__ p, T* __restrict__ out, long long batch, int n0, int n1) {
+  // Gather form of the scatter in gpu.py:40-53: out = S(M p)/12, M = interior mask.
+  const long long total = batch * n0 * n1;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(idx % n1);
+    const int i = static_cast<int>((idx / n1) % n0);
+    auto q = [&](int di, int dj) -> T {
+      const int ii = i + di, jj = j + dj;
+      if (ii < 2 || ii >= n0 - 2 || jj < 2 || jj >= n1 - 2) return T(0);
+      return p[idx + static_cast<long long>(di) * n1 + dj] / T(12);
+    };
+    T val = -T(60) * q(0, 0);
+    val += -q(-2, 0) + T(16) * q(-1, 0) + T(16) * q(1, 0) - q(2, 0);
+    val += -q(0, -2) + T(16) * q(0, -1) + T(16) * q(0, 1) - q(0, 2);
+    out[idx] = val;
+  }
+}
+
+template <typename T>
+__global__ void fold_kernel(const T* __restrict__ g, T* __restrict__ out, long long batch, int nz, int nx, int pad) {
+  const int nzp = nz + 2 * pad, nxp = nx + 2 * pad;
+  const long long total = batch * nz * nx;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(idx % nx);
+    const int z = static_cast<int>((idx / nx) % nz);
+    const T* G = g + (idx / (static_cast<long long>(nz) * nx)) * nzp * nxp;
+    auto at = [&](int i, int j) -> T { return G[static_cast<long long>(i) * nxp + j]; };
+    const int i = pad + z, j = pad + x;
+    T val = at(i, j);
+    const int zi0 = z == 0 ? 0 : (z == nz - 1 ? pad + nz : -1), zi1 = z == 0 ? pad : nzp;
+    const int xj0 = x == 0 ? 0 : (x == nx - 1 ? pad + nx : -1), xj1 = x == 0 ? pad : nxp;
+    if (zi0 >= 0)
+      for (int ii = zi0; ii < zi1; ++ii) val += at(ii, j);
+    if (xj0 >= 0)
+      for (int jj = xj0; jj < xj1; ++jj) val += at(i, jj);
+    if (zi0 >= 0 && xj0 >= 0)
+      for (int ii = zi0; ii < zi1; ++ii)
+        for (int jj = xj0; jj < xj1; ++jj) val += at(ii, jj);
+    out[idx] = val;
+  }
+}
+
+__global__ void mute_kernel(float* __restrict__ out, const float* __restrict__ vmute, int n_models, int n_shots, int nt,
+                            int nx, KParams P) {
+  const long long total = static_cast<long long>(n_models) * n_shots * nt * nx;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(idx % nx);
+    const int t = static_cast<int>((idx / nx) % nt);
+    const int s = static_cast<int>((idx / (static_cast<long long>(nx) * nt)) % n_shots);
+    const int b = static_cast<int>(idx / (static_cast<long long>(nx) * nt * n_shots));
+    out[idx] = mute_weight(t, r, P.shot_cols[s], P.dx, P.dt, vmute[b], P.t_mute);
+  }
+}
+
+__global__ void c2_kernel(const float* __restrict__ vel, float* __restrict__ out, int n_models, int nz, int nx, int pad,
+                          double dtdx2) {
+  const int nzp = nz + 2 * pad, nxp = nx + 2 * pad;
+  const long long total = static_cast<long long>(n_models) * nzp * nxp;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int j = static_cast<int>(idx % nxp);
+    const int i = static_cast<int>((idx / nxp) % nzp);
+    const long long b = idx / (static_cast<long long>(nzp) * nxp);
+    const int vz = min(max(i - pad, 0), nz - 1), vx = min(max(j - pad, 0), nx - 1);
+    const double vp = vel[b * nz * nx + vz * nx + vx];
+    out[idx] = static_cast<float>(vp * vp * dtdx2);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Host side: plans, workspace, launches
+// ----------------------------------------------------------------------------
+struct Plan {
+  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads;
+  size_t smem;
+  int max_clusters;
+  int slots;
+};
+
+int check_geometry(const ss_geometry* g) {
+  if (!g) return fail(SS_ERR_INVALID, "geometry pointer is NULL");
+  if (g->nz < 1 || g->nx < 1 || g->nt < 1) return fail(SS_ERR_INVALID, "nz, nx and nt must be positive");
+  if (g->pad < 2) return fail(SS_ERR_INVALID, "pad must be >= 2");
+  if (g->n_shots < 1 || g->n_shots > SS_MAX_SHOTS) return fail(SS_ERR_INVALID, "n_shots must lie in 1..16");
+  if (g->src_row < 0 || g->src_row >= g->nz) return fail(SS_ERR_INVALID, "src_row outside the model");
+  for (int s = 0; s < g->n_shots; ++s)
+    if (g->shot_cols[s] < 0 || g->shot_cols[s] >= g->nx) return fail(SS_ERR_INVALID, "shot column outside the model");
+  if (!(g->dx > 0.0) || !(g->dt > 0.0) || !(g->r_coef > 0.0) || !(g->r_coef < 1.0) || !(g->vmax_damping > 0.0) ||
+      !(g->amp_ref > 0.0))
+    return fail(SS_ERR_INVALID, "dx, dt, vmax_damping and amp_ref must be positive and 0 < r_coef < 1");
+  return SS_OK;
+}
+
+const void* kernel_for(int mode) {
+  switch (mode) {
+    case SS_MODE_FORWARD: return reinterpret_cast<const void*>(&solve_kernel<SS_MODE_FORWARD>);
+    case SS_MODE_GRADIENT: return reinterpret_cast<const void*>(&solve_kernel<SS_MODE_GRADIENT>);
+    default: return reinterpret_cast<const void*>(&solve_kernel<SS_MODE_IMAGES>);
+  }
+}
+
+size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj) {
+  const size_t field = static_cast<size_t>(bh + 4) * rs;
+  const size_t stage = adj ? static_cast<size_t>(bh) * sw : 0;
+  return (2 * field + 2 * stage + ((nt + 31) & ~31) + 32 + 2 * static_cast<size_t>(nxs)) * sizeof(float) +
+         2 * sizeof(uint64_t);
+}
+
+int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
+  constexpr int H = kRowsPerThread;
+  const bool adj = mode != SS_MODE_FORWARD;
+  p->nzp = g->nz + 2 * g->pad;
+  p->nxp = g->nx + 2 * g->pad;
+  p->ncg = (p->nxp - 4 + 3) / 4;
+  p->rs = 4 * p->ncg + 8;
+  p->sw = 4 * p->ncg;
+  const int nrows = p->nzp - 4;
+  const int max_nseg = kMaxThreads / p->ncg;
+  if (max_nseg < 1) return fail(SS_ERR_UNSUPPORTED, "model too wide for one band of threads");
+  bool ok = false;
+  for (int C = std::max(1, (nrows + max_nseg * H - 1) / (max_nseg * H)); C <= kMaxCluster; ++C) {
+    const int nseg = (nrows + C * H - 1) / (C * H);
+    if (C > 1 && nseg < 1) break;
+    const int bh = nseg * H;
+    if (C > 1 && bh < 2) continue;
+    const size_t sm = smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj);
+    if (sm <= kMaxSmem) {
+      p->C = C;
+      p->nseg = nseg;
+      p->bh = bh;
+      p->smem = sm;
+      ok = true;
+      break;
+    }
+  }
+  if (!ok) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits shared memory for this grid");
+  p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
+  const void* fn = kernel_for(mode);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->smem));
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  if (p->C > 8) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("non-portable cluster: ") + cudaGetErrorString(e));
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = p->C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(p->C, 1, 1);
+  cfg.blockDim = dim3(p->threads, 1, 1);
+  cfg.dynamicSmemBytes = p->smem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  e = cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg);
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaOccupancyMaxActiveClusters: ") + cudaGetErrorString(e));
+  if (nclusters < 1) return fail(SS_ERR_UNSUPPORTED, "no cluster of this plan fits on the device");
+  p->max_clusters = nclusters;
+  p->slots = std::max(1, std::min(nclusters, n_solves));
+  return SS_OK;
+}
+
+inline size_t align_up(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+struct WsLayout {
+  size_t err, hist, trace, gpad, grad, total;
+};
+
+WsLayout ws_layout(const ss_geometry* g, const Plan& p, int mode) {
+  WsLayout w{};
+  size_t off = 0;
+  w.err = off;
+  off = align_up(off + 256);
+  if (mode != SS_MODE_FORWARD) {
+    w.hist = off;
+    off = align_up(off + static_cast<size_t>(p.slots) * g->nt * p.C * p.bh * p.sw * sizeof(float));
+    w.trace = off;
+    off = align_up(off + static_cast<size_t>(p.slots) * g->nt * ((g->nx + 3) & ~3) * sizeof(float));
+    w.gpad = off;
+    off = align_up(off + static_cast<size_t>(p.slots) * std::max(p.nzp * p.nxp, g->nz * g->nx) * sizeof(float));
+    w.grad = off;
+    off = align_up(off + static_cast<size_t>(p.slots) * g->nz * g->nx * sizeof(float));
+  }
+  w.total = off;
+  return w;
+}
+
+KParams base_params(const ss_geometry* g, const Plan& p, int n_models) {
+  KParams k{};
+  k.nz = g->nz;
+  k.nx = g->nx;
+  k.nt = g->nt;
+  k.pad = g->pad;
+  k.nzp = p.nzp;
+  k.nxp = p.nxp;
+  k.n_shots = g->n_shots;
+  k.src_row = g->src_row;
+  for (int s = 0; s < SS_MAX_SHOTS; ++s) k.shot_cols[s] = s < g->n_shots ? g->shot_cols[s] : 0;
+  const double dtdx = g->dt / g->dx;
+  k.dtdx2 = dtdx * dtdx;
+  k.damp_k = 3.0 * g->vmax_damping / (2.0 * g->pad * g->dx) * std::log(1.0 / g->r_coef) * g->dt / 2.0;
+  k.amp_ref = g->amp_ref;
+  k.dx = static_cast<float>(g->dx);
+  k.dt = static_cast<float>(g->dt);
+  k.ncg = p.ncg;
+  k.nseg = p.nseg;
+  k.bh = p.bh;
+  k.C = p.C;
+  k.rs = p.rs;
+  k.sw = p.sw;
+  k.nact = p.ncg * p.nseg;
+  k.nxs = (g->nx + 3) & ~3;
+  k.n_solves = n_models * g->n_shots;
+  return k;
+}
+
+int launch(const Plan& p, int mode, const KParams& k, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = p.C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(p.C * p.slots, 1, 1);
+  cfg.blockDim = dim3(p.threads, 1, 1);
+  cfg.dynamicSmemBytes = p.smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e;
+  switch (mode) {
+    case SS_MODE_FORWARD: e = cudaLaunchKernelEx(&cfg, solve_kernel<SS_MODE_FORWARD>, k); break;
+    case SS_MODE_GRADIENT: e = cudaLaunchKernelEx(&cfg, solve_kernel<SS_MODE_GRADIENT>, k); break;
+    default: e = cudaLaunchKernelEx(&cfg, solve_kernel<SS_MODE_IMAGES>, k); break;
+  }
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaLaunchKernelEx: ") + cudaGetErrorString(e));
+  return SS_OK;
+}
+
+int run_adjoint(int mode, const ss_geometry* g, int n_models, const float* vel, const float* wavelet, const float* obs,
+                const float* v_mute, float t_mute, float eps, int laplacian, float* img, float* illum, float* grad,
+                void* ws, size_t ws_bytes, void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(g);
+  if (rc) return rc;
+  if (n_models < 1) return fail(SS_ERR_INVALID, "n_models must be positive");
+  if (!vel || !wavelet || !obs || !illum) return fail(SS_ERR_INVALID, "vel, wavelet, obs and illum are required");
+  if (mode == SS_MODE_GRADIENT && !grad) return fail(SS_ERR_INVALID, "grad output is required");
+  if (mode == SS_MODE_IMAGES && !img) return fail(SS_ERR_INVALID, "img output is required");
+  if (!(eps > 0.f) && mode == SS_MODE_IMAGES) return fail(SS_ERR_INVALID, "illumination regularization eps must be positive");
+  Plan p;
+  rc = make_plan(g, mode, n_models * g->n_shots, &p);
+  if (rc) return rc;
+  const WsLayout L = ws_layout(g, p, mode);
+  if (!ws || ws_bytes < L.total) return fail(SS_ERR_WORKSPACE, "workspace missing or too small");
+  unsigned char* w = static_cast<unsigned char*>(ws);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SS_CUDA(cudaMemsetAsync(w + L.err, 0, 256, st));
+  KParams k = base_params(g, p, n_models);
+  k.vel = vel;
+  k.wav = wavelet;
+  k.obs = obs;
+  k.vmute = v_mute;
+  k.t_mute = t_mute;
+  k.trace = reinterpret_cast<float*>(w + L.trace);
+  k.illum = illum;
+  k.grad_per_slot = grad == nullptr;
+  k.grad = grad ? grad : reinterpret_cast<float*>(w + L.grad);
+  k.img = img;
+  k.gpad = reinterpret_cast<float*>(w + L.gpad);
+  k.hist = reinterpret_cast<float*>(w + L.hist);
+  k.eps = eps;
+  k.laplacian = laplacian;
+  k.err = reinterpret_cast<int*>(w + L.err);
+  k.ckpt_interval = 1;
+  return launch(p, mode, k, st);
+}
+
+int grid_for(long long total) {
+  return static_cast<int>(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* ss_version(void) { return "shotsweep-b200 0.1.0 (sm_100a)"; }
+
+const char* ss_last_error(void) { return g_last_error.c_str(); }
+
+size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mode) {
+  if (check_geometry(geom) || n_models < 1 || mode < 0 || mode > 2) return 0;
+  Plan p;
+  if (make_plan(geom, mode, n_models * geom->n_shots, &p)) return 0;
+  return ws_layout(geom, p, mode).total;
+}
+
+int32_t ss_workspace_status(const void* workspace, void* stream) {
+  g_last_error.clear();
+  if (!workspace) return fail(SS_ERR_WORKSPACE, "workspace is NULL");
+  int flag = 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SS_CUDA(cudaMemcpyAsync(&flag, workspace, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SS_CUDA(cudaStreamSynchronize(st));
+  if (flag == SS_ERR_NONFINITE) return fail(flag, "observations must be finite");
+  if (flag != 0) return fail(flag, "a device-side bounded wait ran out (history copy did not complete)");
+  return SS_OK;
+}
+
+int32_t ss_plan_info(const ss_geometry* geom, int32_t n_models, int32_t mode, int64_t out[8]) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (!out || n_models < 1) return fail(SS_ERR_INVALID, "bad arguments");
+  Plan p;
+  rc = make_plan(geom, mode, n_models * geom->n_shots, &p);
+  if (rc) return rc;
+  out[0] = p.C;
+  out[1] = p.threads;
+  out[2] = static_cast<int64_t>(p.smem);
+  out[3] = p.bh;
+  out[4] = p.ncg;
+  out[5] = kRowsPerThread;
+  out[6] = p.max_clusters;
+  out[7] = p.slots;
+  return SS_OK;
+}
+
+int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet, float* gathers,
+                   float* ckpt, int32_t ckpt_interval, void* workspace, size_t workspace_bytes, void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (n_models < 1) return fail(SS_ERR_INVALID, "n_models must be positive");
+  if (!vel || !wavelet || !gathers) return fail(SS_ERR_INVALID, "vel, wavelet and gathers are required");
+  if (ckpt && ckpt_interval < 1) return fail(SS_ERR_INVALID, "ckpt_interval must be positive");
+  Plan p;
+  rc = make_plan(geom, SS_MODE_FORWARD, n_models * geom->n_shots, &p);
+  if (rc) return rc;
+  const WsLayout L = ws_layout(geom, p, SS_MODE_FORWARD);
+  if (!workspace || workspace_bytes < L.total) return fail(SS_ERR_WORKSPACE, "workspace missing or too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SS_CUDA(cudaMemsetAsync(workspace, 0, 256, st));
+  KParams k = base_params(geom, p, n_models);
+  k.vel = vel;
+  k.wav = wavelet;
+  k.gathers = gathers;
+  k.ckpt = ckpt;
+  k.ckpt_interval = ckpt ? ckpt_interval : 1;
+  k.n_ckpt = ckpt ? (geom->nt + ckpt_interval - 1) / ckpt_interval : 0;
+  k.err = static_cast<int*>(workspace);
+  return launch(p, SS_MODE_FORWARD, k, st);
+}
+
+int32_t ss_gradient(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                    const float* obs, const float* v_mute, float t_mute, float* grad, float* illum, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+  return run_adjoint(SS_MODE_GRADIENT, geom, n_models, vel, wavelet, obs, v_mute, t_mute, 1.f, 0, nullptr, illum,
+                     grad, workspace, workspace_bytes, stream);
+}
+
+int32_t ss_images(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet, const float* obs,
+                  const float* v_mute, float t_mute, float eps, int32_t laplacian, float* img, float* illum,
+                  float* grad, void* workspace, size_t workspace_bytes, void* stream) {
+  return run_adjoint(SS_MODE_IMAGES, geom, n_models, vel, wavelet, obs, v_mute, t_mute, eps, laplacian, img, illum,
+                     grad, workspace, workspace_bytes, stream);
+}
+
+#define SS_ELEMENTWISE(NAME, T, KERNEL)                                                                  \
+  int32_t NAME(const T* p, T* out, int64_t batch, int32_t n0, int32_t n1, void* stream) {               \
+    g_last_error.clear();                                                                               \
+    if (!p || !out || batch < 0 || n0 < 1 || n1 < 1) return fail(SS_ERR_INVALID, "bad arguments");      \
+    const long long total = static_cast<long long>(batch) * n0 * n1;                                    \
+    if (total == 0) return SS_OK;                                                                        \
+    KERNEL<T><<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(p, out, batch, n0, n1);   \
+    SS_CUDA(cudaGetLastError());                                                                        \
+    return SS_OK;                                                                                        \
+  }
+SS_ELEMENTWISE(ss_lap_f32, float, lap_kernel)
+SS_ELEMENTWISE(ss_lap_f64, double, lap_kernel)
+SS_ELEMENTWISE(ss_lap_adjoint_f32, float, lap_adjoint_kernel)
+SS_ELEMENTWISE(ss_lap_adjoint_f64, double, lap_adjoint_kernel)
+#undef SS_ELEMENTWISE
+
+#define SS_FOLD(NAME, T)                                                                                      \
+  int32_t NAME(const T* g, T* out, int64_t batch, int32_t nz, int32_t nx, int32_t pad, void* stream) {       \
+    g_last_error.clear();                                                                                    \
+    if (!g || !out || batch < 0 || nz < 1 || nx < 1 || pad < 0) return fail(SS_ERR_INVALID, "bad arguments"); \
+    const long long total = static_cast<long long>(batch) * nz * nx;                                         \
+    if (total == 0) return SS_OK;                                                                             \
+    fold_kernel<T><<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(g, out, batch, nz, nx, pad); \
+    SS_CUDA(cudaGetLastError());                                                                             \
+    return SS_OK;                                                                                             \
+  }
+SS_FOLD(ss_fold_edge_padding_f32, float)
+SS_FOLD(ss_fold_edge_padding_f64, double)
+#undef SS_FOLD
+
+int32_t ss_mute_weights(const ss_geometry* geom, int32_t n_models, const float* v_mute, float t_mute, float* out,
+                        void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (!v_mute || !out || n_models < 0) return fail(SS_ERR_INVALID, "bad arguments");
+  const long long total = static_cast<long long>(n_models) * geom->n_shots * geom->nt * geom->nx;
+  if (total == 0) return SS_OK;
+  KParams k{};
+  for (int s = 0; s < SS_MAX_SHOTS; ++s) k.shot_cols[s] = s < geom->n_shots ? geom->shot_cols[s] : 0;
+  k.dx = static_cast<float>(geom->dx);
+  k.dt = static_cast<float>(geom->dt);
+  k.t_mute = t_mute;
+  mute_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, v_mute, n_models, geom->n_shots,
+                                                                              geom->nt, geom->nx, k);
+  SS_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_c2_field(const ss_geometry* geom, int32_t n_models, const float* vel, float* out, void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (!vel || !out || n_models < 0) return fail(SS_ERR_INVALID, "bad arguments");
+  const long long total = static_cast<long long>(n_models) * (geom->nz + 2 * geom->pad) * (geom->nx + 2 * geom->pad);
+  if (total == 0) return SS_OK;
+  const double dtdx = geom->dt / geom->dx;
+  c2_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(vel, out, n_models, geom->nz, geom->nx,
+                                                                           geom->pad, dtdx * dtdx);
+  SS_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,168 @@
+"""Geometry-generic device entry points over the C ABI.
+
+``Engine(geometry)`` runs forward modelling, gradients and RTM images for any
+grid / time axis / shot layout that the kernels plan for (the reference's
+``Sim`` hard-wires 70x70, 1000 steps, 5 shots; ``shotsweep_b200.gpu.Sim`` is a
+thin layer over this class with that geometry).  Arguments are CUDA float32
+tensors; outputs are new CUDA tensors.  The per-step history workspace is
+allocated once and reused while it is large enough.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def geometry(nz=70, nx=70, nt=1000, pad=40, shot_cols=(0, 17, 34, 52, 69), src_row=1, dx=10.0, dt=1e-3,
+             R=1e-5):
+    return _lib.make_geometry(nz, nx, nt, pad, shot_cols, src_row, dx, dt, R)
+
+
+class Engine:
+    def __init__(self, geom, device=None):
+        self.g = geom
+        self.device = torch.device('cuda') if device is None else torch.device(device)
+        _lib.require_cuda(self.device)
+        self.L = _lib.load()
+        self._ws = None
+
+    # -- plumbing -----------------------------------------------------------
+    @property
+    def shape(self):
+        return self.g.nz, self.g.nx
+
+    @property
+    def n_shots(self):
+        return self.g.n_shots
+
+    @property
+    def padded(self):
+        return self.g.nz + 2 * self.g.pad, self.g.nx + 2 * self.g.pad
+
+    def plan(self, n_models, mode):
+        out = (ctypes.c_int64 * 8)()
+        with torch.cuda.device(self.device):
+            _lib.check(self.L.ss_plan_info(ctypes.byref(self.g), n_models, mode, out), 'ss_plan_info')
+        keys = ('cluster', 'threads', 'smem', 'band_rows', 'col_groups', 'rows_per_thread', 'max_clusters', 'slots')
+        return dict(zip(keys, list(out)))
+
+    def workspace(self, n_models, mode):
+        with torch.cuda.device(self.device):
+            need = self.L.ss_workspace_bytes(ctypes.byref(self.g), n_models, mode)
+        if need == 0:
+            _lib.check(_lib.ERR_UNSUPPORTED, 'ss_workspace_bytes')
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = None
+            self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def _stream(self):
+        return _lib.stream_handle(self.device)
+
+    def _check_in(self, t, shape, name):
+        if not isinstance(t, torch.Tensor) or t.device != self.device or t.dtype != torch.float32:
+            raise ValueError(f'{name} must be a float32 tensor on {self.device}')
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f'{name} must have shape {tuple(shape)}, got {tuple(t.shape)}')
+        return t.contiguous()
+
+    def status(self):
+        """Raise if the last simulation on this engine recorded a device-side failure."""
+        if self._ws is None:
+            return
+        with torch.cuda.device(self.device):
+            rc = self.L.ss_workspace_status(_lib.ptr(self._ws), self._stream())
+        if rc == _lib.ERR_NONFINITE:
+            raise ValueError('observations must be finite')
+        _lib.check(rc, 'device status')
+
+    # -- entry points ----------------------------------------------------------
+    def forward(self, vel, wavelet, ckpt_interval=None, out=None):
+        """Gathers [B, S, nt, nx] (+ checkpoints [B, S, n_ck, 2, nzp, nxp] if ckpt_interval)."""
+        g = self.g
+        B = vel.shape[0]
+        vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
+        wavelet = self._check_in(wavelet, (g.nt,), 'wavelet')
+        if out is None:
+            out = torch.empty(B, g.n_shots, g.nt, g.nx, dtype=torch.float32, device=self.device)
+        ck = None
+        if ckpt_interval:
+            n_ck = math.ceil(g.nt / ckpt_interval)
+            ck = torch.zeros(B, g.n_shots, n_ck, 2, *self.padded, dtype=torch.float32, device=self.device)
+        ws = self.workspace(B, _lib.MODE_FORWARD)
+        with torch.cuda.device(self.device):
+            _lib.check(self.L.ss_forward(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(out),
+                                         _lib.ptr(ck), int(ckpt_interval or 0), _lib.ptr(ws), ws.numel(),
+                                         self._stream()), 'ss_forward')
+        return (out, ck) if ckpt_interval else out
+
+    def gradient(self, vel, wavelet, obs, v_mute=None, t_mute=0.12):
+        """(grad, illum), each [B, S, nz, nx]."""
+        g = self.g
+        B = vel.shape[0]
+        vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
+        wavelet = self._check_in(wavelet, (g.nt,), 'wavelet')
+        obs = self._check_in(obs, (B, g.n_shots, g.nt, g.nx), 'obs')
+        if v_mute is not None:
+            v_mute = self._check_in(v_mute, (B,), 'v_mute')
+        grad = torch.empty(B, g.n_shots, g.nz, g.nx, dtype=torch.float32, device=self.device)
+        illum = torch.empty_like(grad)
+        ws = self.workspace(B, _lib.MODE_GRADIENT)
+        with torch.cuda.device(self.device):
+            _lib.check(self.L.ss_gradient(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(obs),
+                                          _lib.ptr(v_mute), float(t_mute), _lib.ptr(grad), _lib.ptr(illum),
+                                          _lib.ptr(ws), ws.numel(), self._stream()), 'ss_gradient')
+        return grad, illum
+
+    def images(self, vel, wavelet, obs, v_mute=None, t_mute=0.12, eps=1e-4, laplacian=True, want_grad=False,
+               out=None):
+        """(img, illum[, grad]), each [B, S, nz, nx]."""
+        if not eps > 0:
+            raise ValueError('illumination regularization eps must be positive')
+        g = self.g
+        B = vel.shape[0]
+        vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
+        wavelet = self._check_in(wavelet, (g.nt,), 'wavelet')
+        obs = self._check_in(obs, (B, g.n_shots, g.nt, g.nx), 'obs')
+        if v_mute is not None:
+            v_mute = self._check_in(v_mute, (B,), 'v_mute')
+        if out is None:
+            img = torch.empty(B, g.n_shots, g.nz, g.nx, dtype=torch.float32, device=self.device)
+            illum = torch.empty_like(img)
+        else:
+            img, illum = out
+        grad = torch.empty_like(img) if want_grad else None
+        ws = self.workspace(B, _lib.MODE_IMAGES)
+        with torch.cuda.device(self.device):
+            _lib.check(self.L.ss_images(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(obs),
+                                        _lib.ptr(v_mute), float(t_mute), float(eps), int(bool(laplacian)),
+                                        _lib.ptr(img), _lib.ptr(illum), _lib.ptr(grad), _lib.ptr(ws), ws.numel(),
+                                        self._stream()), 'ss_images')
+        return (img, illum, grad) if want_grad else (img, illum)
+
+    def mute_weights(self, v_mute, t_mute=0.12):
+        g = self.g
+        v_mute = self._check_in(v_mute, (v_mute.shape[0],), 'v_mute')
+        out = torch.empty(v_mute.shape[0], g.n_shots, g.nt, g.nx, dtype=torch.float32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.L.ss_mute_weights(ctypes.byref(g), v_mute.shape[0], _lib.ptr(v_mute), float(t_mute),
+                                              _lib.ptr(out), self._stream()), 'ss_mute_weights')
+        return out
+
+    def c2_field(self, vel):
+        g = self.g
+        out = torch.empty(vel.shape[0], *self.padded, dtype=torch.float32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.L.ss_c2_field(ctypes.byref(g), vel.shape[0], _lib.ptr(vel), _lib.ptr(out),
+                                          self._stream()), 'ss_c2_field')
+        return out
+
+
+def scaled_wavelet(wavelet, device):
+    """The reference injects wavelet*1e3 (gpu.py:94), computed in float64 then cast."""
+    return torch.as_tensor(np.asarray(wavelet, np.float64) * 1e3, dtype=torch.float32).to(device)

@@ -1,0 +1,74 @@
+"""The CPU oracle against golden vectors that the reference itself produced (tests/golden)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+from .conftest import golden
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+def test_small_operators_match_reference():
+    g = golden('ops_small')
+    x, y = torch.from_numpy(g['x']), torch.from_numpy(g['y'])
+    np.testing.assert_allclose(O.lap(x).numpy(), g['lap_x'], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(O.lap_adjoint(y).numpy(), g['lapT_y'], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(O.fold_edge_padding(torch.from_numpy(g['big']), 40).numpy(), g['fold_big'],
+                               rtol=1e-12, atol=1e-10)
+    np.testing.assert_allclose(O.ricker(), g['ricker'], rtol=0, atol=1e-15)
+    assert O.shot_columns(70, 5) == tuple(g['src'])
+    sim = O.OracleSim()
+    mute = sim.mute_weights(g['mute_v']).numpy()[:, :, ::7, :]
+    np.testing.assert_allclose(mute, g['mute_sub'], rtol=0, atol=1e-7)
+
+
+def test_laplacian_transpose_including_boundary():
+    gen = torch.Generator().manual_seed(3)
+    x = torch.randn(3, 13, 17, generator=gen, dtype=torch.float64)
+    y = torch.randn(3, 13, 17, generator=gen, dtype=torch.float64)
+    assert abs(float((O.lap(x) * y).sum() - (x * O.lap_adjoint(y)).sum())) < 1e-10
+
+
+@pytest.fixture(scope='module')
+def plain():
+    return golden('plain_small')
+
+
+def test_oracle_gathers_match_reference(plain):
+    sim = O.OracleSim()
+    out = sim.gathers(plain['model'][None].astype(np.float64))[0]
+    assert rel(out, plain['gathers']) < 1e-6      # fixture stored as float32
+
+
+def test_oracle_images_gradient_match_reference(plain):
+    sim = O.OracleSim()
+    bgs = plain['backgrounds']
+    obs = np.repeat(plain['gathers'][None].astype(np.float64), 3, 0)
+    mute = np.full(3, float(plain['v_surface']))
+    grad, illum = sim.gradient(bgs, obs, v_mute=mute)
+    assert rel(grad, plain['grad']) < 1e-6
+    assert rel(illum, plain['illum']) < 1e-6
+    img = O.image_epilogue(torch.from_numpy(grad), torch.from_numpy(illum)).numpy()
+    assert rel(img, plain['images']) < 1e-6
+    img_nl = O.image_epilogue(torch.from_numpy(grad), torch.from_numpy(illum), laplacian=False).numpy()
+    assert rel(img_nl, plain['images_nolap']) < 1e-6
+
+
+def test_oracle_inverse_crime_gradients_match_reference():
+    g = golden('fd_small')
+    sim = O.OracleSim()
+    grad, illum = sim.gradient(g['velocity'], g['observed'].astype(np.float64))
+    assert rel(grad, g['grad']) < 1e-6 and rel(illum, g['illum']) < 1e-6
+    grad, illum = sim.gradient(g['velocity'], g['observed'].astype(np.float64), v_mute=np.array([2000.0]))
+    assert rel(grad, g['grad_muted']) < 1e-6 and rel(illum, g['illum_muted']) < 1e-6
+
+
+def test_oracle_background_helpers(plain):
+    from shotsweep_b200 import synth
+    trend = O.depth_trend(synth.population(500))
+    np.testing.assert_allclose(trend, plain['trend'], rtol=1e-12)
+    np.testing.assert_allclose(O.backgrounds(float(plain['v_surface']), trend), plain['backgrounds'], rtol=1e-12)
