@@ -39,9 +39,10 @@
 
 namespace {
 
-constexpr int kRowsPerThread = 6;          // H: rows per thread in the band
-constexpr int kMaxThreads = 512;           // register budget: 128 regs/thread
+constexpr int kRowsPerThread = 5;          // H: rows per thread in the band
+constexpr int kMaxThreads = 384;           // register budget: 168 regs/thread
 constexpr int kMaxCluster = 16;
+constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush
 constexpr size_t kMaxSmem = 227 * 1024;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s per bounded wait
 
@@ -193,6 +194,7 @@ struct Smem {
   float* wav;
   float* red;
   float* res[2];   // residual row of the current / next adjoint step
+  float* trc;      // ring of kTraceRing receiver rows, flushed to global memory
   uint64_t* bar;
 };
 
@@ -205,351 +207,12 @@ __device__ __forceinline__ float mute_weight(int t, int r, int shot_col, float d
   return 0.5f - 0.5f * cosf(3.14159265358979323846f * ramp);
 }
 
+// Fold the padded gradient onto the model edges (gpu.py:56-67, 185-187) and,
+// for images, normalise by illumination and Laplacian-filter (gpu.py:206-209).
+// Called by every thread of the cluster; gp holds this slot's padded gradient.
 template <int MODE>
-__global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) {
-  constexpr int H = kRowsPerThread;
-  constexpr bool ADJ = MODE != SS_MODE_FORWARD;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-
-  const int tid = threadIdx.x;
-  const int nthr = blockDim.x;
-  const int rank = static_cast<int>(cluster_rank());
-  const int slot = static_cast<int>(cluster_id());
-  const int n_slots = static_cast<int>(cluster_count());
-
-  // ---- shared-memory carve-up (identical in every CTA of the cluster) ----
-  Smem S;
-  {
-    const size_t field = static_cast<size_t>(P.bh + 4) * P.rs;
-    const size_t stage = ADJ ? static_cast<size_t>(P.bh) * P.sw : 0;
-    float* base = reinterpret_cast<float*>(smem_raw);
-    S.f[0] = base;
-    S.f[1] = base + field;
-    S.stg[0] = base + 2 * field;
-    S.stg[1] = base + 2 * field + stage;
-    S.wav = base + 2 * field + 2 * stage;
-    S.red = S.wav + ((P.nt + 31) & ~31);
-    S.res[0] = S.red + 32;
-    S.res[1] = S.res[0] + P.nxs;
-    S.bar = reinterpret_cast<uint64_t*>(S.res[1] + P.nxs);
-  }
-  for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
-  if (ADJ && tid == 0) {
-    mbar_init(smem_u32(&S.bar[0]), 1);
-    mbar_init(smem_u32(&S.bar[1]), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  uint32_t phase_bits = 0;   // parity of the next wait on each staging buffer
-
-  // ---- this thread's block of cells: H rows x 4 columns -----------------
-  const bool active = tid < P.nact;
-  const int cg = active ? tid % P.ncg : 0;
-  const int seg = active ? tid / P.ncg : 0;
-  const int row0 = 2 + rank * P.bh;               // first padded row of the band
-  const int myrow = row0 + seg * H;               // first padded row of this thread
-  const int col0 = 2 + 4 * cg;                    // first padded column
-  const int o0 = 4 * cg + 4;                      // shared-memory column offset of col0
-  const int lr0 = seg * H;                        // shared row of window row k=-2
-  const int src_r = P.pad + P.src_row;            // padded row of sources and receivers
-  const int rec_rank = (src_r - 2) / P.bh;
-
-  // Halo pushes to the neighbouring bands (rows needed by their stencils).
-  const bool push_up = active && seg == 0 && rank > 0;
-  const bool push_dn = active && seg == P.nseg - 1 && rank < P.C - 1;
-  // Remote addresses in buffer 0; buffer 1 lies field_bytes further on.
-  const uint32_t field_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh + 4) * P.rs * sizeof(float));
-  const uint32_t up_addr = push_up ? mapa(smem_u32(S.f[0] + (P.bh + 2) * P.rs + o0), rank - 1) : 0u;
-  const uint32_t dn_addr = push_dn ? mapa(smem_u32(S.f[0] + o0), rank + 1) : 0u;
-
-  const int rec_k = (active && src_r >= myrow && src_r < myrow + H) ? src_r - myrow : -1;
-
-  const size_t field_floats = static_cast<size_t>(P.bh + 4) * P.rs;
-  const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * P.sw * sizeof(float));
-  const size_t hist_slot = static_cast<size_t>(P.nt) * P.C * P.bh * P.sw;
-  float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * P.sw
-                               : nullptr;
-  const size_t hist_step = static_cast<size_t>(P.C) * P.bh * P.sw;
-
-  cluster_sync();   // barriers initialised and wavelet staged everywhere
-
-  for (int solve = slot; solve < P.n_solves; solve += n_slots) {
-    const int b = solve / P.n_shots;
-    const int s = solve - b * P.n_shots;
-    const float* v = P.vel + static_cast<size_t>(b) * P.nz * P.nx;
-    const int shot_col = P.shot_cols[s];
-    const int src_c = P.pad + shot_col;
-
-    // ---- per-cell coefficients ----------------------------------------
-    float kap[H][4], sig[H][4], acc[H][4];
-#pragma unroll
-    for (int k = 0; k < H; ++k) {
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int r = myrow + k, c = col0 + m;
-        kap[k][m] = 0.f;
-        sig[k][m] = 0.f;
-        acc[k][m] = 0.f;
-        if (active && r < P.nzp - 2 && c < P.nxp - 2) {
-          const double dz = layer_depth(r, P.nzp, P.pad), dxl = layer_depth(c, P.nxp, P.pad);
-          const float A = static_cast<float>(1.0 / (1.0 + P.damp_k * (dz * dz + dxl * dxl)));
-          const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
-          const double vp = v[vz * P.nx + vx];
-          const float c2 = static_cast<float>(vp * vp * P.dtdx2);
-          kap[k][m] = 2.f * A;
-          sig[k][m] = (c2 * A) / 12.f;
-        }
-      }
-    }
-    int src_k = -1, src_m = 0;
-    if (active && src_r >= myrow && src_r < myrow + H && src_c >= col0 && src_c < col0 + 4) {
-      src_k = src_r - myrow;
-      src_m = src_c - col0;
-    }
-    const double v_src = v[P.src_row * P.nx + shot_col];
-    const float amp = static_cast<float>((v_src / P.amp_ref) * (v_src / P.amp_ref));
-
-    const int tstride = (MODE == SS_MODE_FORWARD) ? P.nx : P.nxs;
-    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + static_cast<size_t>(solve) * P.nt * P.nx
-                                             : P.trace + static_cast<size_t>(slot) * P.nt * P.nxs;
-
-    // ---- zero both wavefields (own rows and halos) ---------------------
-    for (size_t i = tid; i < field_floats / 2; i += nthr) {
-      reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
-      reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
-    }
-    cluster_sync();
-
-    // ================= forward: t = 0 .. nt-1 =============================
-    int cur = 0;   // S.f[cur] = p[t], S.f[cur^1] = p[t-1]
-    for (int t = 0; t < P.nt; ++t) {
-      const float* X = cur ? S.f[1] : S.f[0];
-      float* Y = cur ? S.f[0] : S.f[1];
-      if (MODE == SS_MODE_FORWARD && P.ckpt != nullptr && t % P.ckpt_interval == 0 && active) {
-        float* ck = P.ckpt + ((static_cast<size_t>(solve) * P.n_ckpt + t / P.ckpt_interval) * 2) * P.nzp * P.nxp;
-#pragma unroll
-        for (int k = 0; k < H; ++k) {
-          const int r = myrow + k;
-          if (r >= P.nzp - 2) break;
-#pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            const int c = col0 + m;
-            if (c < P.nxp - 2) {
-              ck[static_cast<size_t>(r) * P.nxp + c] = Y[(lr0 + k + 2) * P.rs + o0 + m];
-              ck[static_cast<size_t>(P.nzp) * P.nxp + static_cast<size_t>(r) * P.nxp + c] =
-                  X[(lr0 + k + 2) * P.rs + o0 + m];
-            }
-          }
-        }
-      }
-      if (active) {
-        const float wt = S.wav[t] * amp;
-        const float* xc = X + lr0 * P.rs + o0;
-        float4 r0 = *reinterpret_cast<const float4*>(xc);
-        float4 r1 = *reinterpret_cast<const float4*>(xc + P.rs);
-        float4 r2 = *reinterpret_cast<const float4*>(xc + 2 * P.rs);
-        float4 r3 = *reinterpret_cast<const float4*>(xc + 3 * P.rs);
-        float* stg = ADJ ? ((t & 1) ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg : nullptr;
-#pragma unroll
-        for (int k = 0; k < H; ++k) {
-          const float4 r4 = *reinterpret_cast<const float4*>(xc + (k + 4) * P.rs);
-          const float* rowc = xc + (k + 2) * P.rs;
-          const float2 lf = *reinterpret_cast<const float2*>(rowc - 2);
-          const float2 rt = *reinterpret_cast<const float2*>(rowc + 4);
-          float4 L;
-          L.x = stencil(r0.x, r1.x, r2.x, r3.x, r4.x, lf.x, lf.y, r2.y, r2.z);
-          L.y = stencil(r0.y, r1.y, r2.y, r3.y, r4.y, lf.y, r2.x, r2.z, r2.w);
-          L.z = stencil(r0.z, r1.z, r2.z, r3.z, r4.z, r2.x, r2.y, r2.w, rt.x);
-          L.w = stencil(r0.w, r1.w, r2.w, r3.w, r4.w, r2.y, r2.z, rt.x, rt.y);
-          float* yp = Y + (lr0 + k + 2) * P.rs + o0;
-          const float4 p0 = *reinterpret_cast<const float4*>(yp);
-          float4 p2;
-          p2.x = fmaf(sig[k][0], L.x, fmaf(kap[k][0], r2.x - p0.x, p0.x));
-          p2.y = fmaf(sig[k][1], L.y, fmaf(kap[k][1], r2.y - p0.y, p0.y));
-          p2.z = fmaf(sig[k][2], L.z, fmaf(kap[k][2], r2.z - p0.z, p0.z));
-          p2.w = fmaf(sig[k][3], L.w, fmaf(kap[k][3], r2.w - p0.w, p0.w));
-          if (k == src_k) {   // injection after damping (gpu.py:113-114)
-            if (src_m == 0) p2.x += wt;
-            else if (src_m == 1) p2.y += wt;
-            else if (src_m == 2) p2.z += wt;
-            else p2.w += wt;
-          }
-          *reinterpret_cast<float4*>(yp) = p2;
-          if (push_up && k < 2) st_cluster_v4(up_addr + (cur ^ 1) * field_bytes + 4u * (k * P.rs), p2);
-          if (push_dn && k >= H - 2)
-            st_cluster_v4(dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * P.rs), p2);
-          if (ADJ) {
-            *reinterpret_cast<float4*>(stg + k * P.sw) = L;
-            acc[k][0] = fmaf(L.x, L.x, acc[k][0]);
-            acc[k][1] = fmaf(L.y, L.y, acc[k][1]);
-            acc[k][2] = fmaf(L.z, L.z, acc[k][2]);
-            acc[k][3] = fmaf(L.w, L.w, acc[k][3]);
-          }
-          if (k == rec_k) {   // receivers at every model column (gpu.py:134)
-            float* tr = trace + static_cast<size_t>(t) * tstride + (col0 - P.pad);
-            const int rr = col0 - P.pad;
-            if (rr >= 0 && rr < P.nx) tr[0] = p2.x;
-            if (rr + 1 >= 0 && rr + 1 < P.nx) tr[1] = p2.y;
-            if (rr + 2 >= 0 && rr + 2 < P.nx) tr[2] = p2.z;
-            if (rr + 3 >= 0 && rr + 3 < P.nx) tr[3] = p2.w;
-          }
-          r0 = r1;
-          r1 = r2;
-          r2 = r3;
-          r3 = r4;
-        }
-      }
-      if (ADJ) {
-        fence_proxy_async_smem();
-        if (tid == 0 && t > 0) bulk_wait_read_all();   // store of step t-1 has left shared memory
-      }
-      cluster_sync();
-      if (ADJ && tid == 0)
-        bulk_store(hist_mine + static_cast<size_t>(t) * hist_step, smem_u32((t & 1) ? S.stg[1] : S.stg[0]), stage_bytes);
-      cur ^= 1;
-    }
-
-    if (MODE == SS_MODE_FORWARD) continue;
-
-    // ---- forward epilogue: illumination = sum_t (S/12)^2 on model cells --
-    if (tid == 0) {
-      bulk_wait_all();
-      fence_proxy_async_all();
-    }
-    {
-      float* il = P.illum + static_cast<size_t>(solve) * P.nz * P.nx;
-#pragma unroll
-      for (int k = 0; k < H; ++k)
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const int z = myrow + k - P.pad, x = col0 + m - P.pad;
-          if (active && z >= 0 && z < P.nz && x >= 0 && x < P.nx)
-            il[z * P.nx + x] = acc[k][m] * (1.f / 144.f);
-          acc[k][m] = 0.f;
-        }
-    }
-    // ---- residual (sim - obs) * mute, in place over the trace ------------
-    if (rank == rec_rank) {
-      const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * P.nx;
-      const float vm = P.vmute ? P.vmute[b] : 0.f;
-      for (int i = tid; i < P.nt * P.nx; i += nthr) {
-        const int t = i / P.nx, r = i - t * P.nx;
-        const float o = ob[i];
-        if (!isfinite(o)) atomicExch(P.err, static_cast<int>(SS_ERR_NONFINITE));
-        float res = trace[t * P.nxs + r] - o;
-        if (P.vmute) res *= mute_weight(t, r, shot_col, P.dx, P.dt, vm, P.t_mute);
-        trace[t * P.nxs + r] = res;
-      }
-      fence_proxy_async_all();   // these rows are read back by bulk copies
-      __syncthreads();
-    }
-
-    // ================= adjoint: t = nt-1 .. 0 =============================
-    for (size_t i = tid; i < field_floats / 2; i += nthr) {
-      reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
-      reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
-    }
-    float src_acc = 0.f;
-    const bool res_here = rank == rec_rank;
-    const uint32_t res_bytes = static_cast<uint32_t>(P.nxs * sizeof(float));
-    // One bulk copy brings the history slab of step t, one more (on the band
-    // with the receivers) the residual row of step t; both signal bar[t&1].
-    auto issue = [&](int t) {
-      const int bi = t & 1;
-      const uint32_t bar = smem_u32(&S.bar[0]) + 8u * bi;
-      mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
-      bulk_load(smem_u32(bi ? S.stg[1] : S.stg[0]), hist_mine + static_cast<size_t>(t) * hist_step, stage_bytes, bar);
-      if (res_here) bulk_load(smem_u32(bi ? S.res[1] : S.res[0]), trace + static_cast<size_t>(t) * P.nxs, res_bytes, bar);
-    };
-    cluster_sync();
-    if (tid == 0) issue(P.nt - 1);
-    cur = 0;   // S.f[cur] = th[t+1], S.f[cur^1] = th[t+2]
-    for (int t = P.nt - 1; t >= 0; --t) {
-      const float* X = cur ? S.f[1] : S.f[0];
-      float* Y = cur ? S.f[0] : S.f[1];
-      if (tid == 0 && t > 0) issue(t - 1);
-      const int bi = t & 1;
-      mbar_wait_bounded(smem_u32(&S.bar[0]) + 8u * bi, (phase_bits >> bi) & 1u, P.err);
-      phase_bits ^= 1u << bi;
-      if (active) {
-        const float wt = S.wav[t];
-        const float* xc = X + lr0 * P.rs + o0;
-        const float* hl = (bi ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg;
-        float4 r0 = *reinterpret_cast<const float4*>(xc);
-        float4 r1 = *reinterpret_cast<const float4*>(xc + P.rs);
-        float4 r2 = *reinterpret_cast<const float4*>(xc + 2 * P.rs);
-        float4 r3 = *reinterpret_cast<const float4*>(xc + 3 * P.rs);
-#pragma unroll
-        for (int k = 0; k < H; ++k) {
-          const float4 r4 = *reinterpret_cast<const float4*>(xc + (k + 4) * P.rs);
-          const float* rowc = xc + (k + 2) * P.rs;
-          const float2 lf = *reinterpret_cast<const float2*>(rowc - 2);
-          const float2 rt = *reinterpret_cast<const float2*>(rowc + 4);
-          float4 L;
-          L.x = stencil(r0.x, r1.x, r2.x, r3.x, r4.x, lf.x, lf.y, r2.y, r2.z);
-          L.y = stencil(r0.y, r1.y, r2.y, r3.y, r4.y, lf.y, r2.x, r2.z, r2.w);
-          L.z = stencil(r0.z, r1.z, r2.z, r3.z, r4.z, r2.x, r2.y, r2.w, rt.x);
-          L.w = stencil(r0.w, r1.w, r2.w, r3.w, r4.w, r2.y, r2.z, rt.x, rt.y);
-          float* yp = Y + (lr0 + k + 2) * P.rs + o0;
-          const float4 q2 = *reinterpret_cast<const float4*>(yp);
-          float4 q;
-          q.x = fmaf(sig[k][0], L.x, fmaf(kap[k][0], r2.x - q2.x, q2.x));
-          q.y = fmaf(sig[k][1], L.y, fmaf(kap[k][1], r2.y - q2.y, q2.y));
-          q.z = fmaf(sig[k][2], L.z, fmaf(kap[k][2], r2.z - q2.z, q2.z));
-          q.w = fmaf(sig[k][3], L.w, fmaf(kap[k][3], r2.w - q2.w, q2.w));
-          if (k == rec_k) {   // residual injection on the receiver row (gpu.py:180)
-            const float* rs = bi ? S.res[1] : S.res[0];
-            const int rr = col0 - P.pad;
-            if (rr >= 0 && rr < P.nx) q.x = fmaf(sig[k][0], rs[rr], q.x);
-            if (rr + 1 >= 0 && rr + 1 < P.nx) q.y = fmaf(sig[k][1], rs[rr + 1], q.y);
-            if (rr + 2 >= 0 && rr + 2 < P.nx) q.z = fmaf(sig[k][2], rs[rr + 2], q.z);
-            if (rr + 3 >= 0 && rr + 3 < P.nx) q.w = fmaf(sig[k][3], rs[rr + 3], q.w);
-          }
-          *reinterpret_cast<float4*>(yp) = q;
-          if (push_up && k < 2) st_cluster_v4(up_addr + (cur ^ 1) * field_bytes + 4u * (k * P.rs), q);
-          if (push_dn && k >= H - 2)
-            st_cluster_v4(dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * P.rs), q);
-          const float4 h = *reinterpret_cast<const float4*>(hl + k * P.sw);
-          acc[k][0] = fmaf(q.x, h.x, acc[k][0]);
-          acc[k][1] = fmaf(q.y, h.y, acc[k][1]);
-          acc[k][2] = fmaf(q.z, h.z, acc[k][2]);
-          acc[k][3] = fmaf(q.w, h.w, acc[k][3]);
-          if (k == src_k) {   // source-strength derivative (gpu.py:182)
-            const float qs = src_m == 0 ? q.x : src_m == 1 ? q.y : src_m == 2 ? q.z : q.w;
-            src_acc = fmaf(qs, wt, src_acc);
-          }
-          r0 = r1;
-          r1 = r2;
-          r2 = r3;
-          r3 = r4;
-        }
-      }
-      cluster_sync();
-      cur ^= 1;
-    }
-
-    // ---- padded gradient 2/v * sum_t th*S(p), plus the source term -------
-    float* gp = P.gpad + static_cast<size_t>(slot) * P.nzp * P.nxp;
-    if (active) {
-#pragma unroll
-      for (int k = 0; k < H; ++k)
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const int r = myrow + k, c = col0 + m;
-          if (r < P.nzp - 2 && c < P.nxp - 2) {
-            const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
-            const float vp = v[vz * P.nx + vx];
-            float gval = 2.f * acc[k][m] / vp;
-            if (k == src_k && m == src_m) {
-              const float deriv = static_cast<float>(2.0 * v_src / (P.amp_ref * P.amp_ref));
-              gval += src_acc * deriv / sig[k][m];
-            }
-            gp[static_cast<size_t>(r) * P.nxp + c] = gval;
-          }
-        }
-    }
-    __threadfence();
-    cluster_sync();
-
+__device__ __forceinline__ void epilogue(const KParams& P, Smem& S, float* gp, int solve, int slot, int rank, int tid,
+                                         int nthr) {
     // ---- fold the padding onto the edge cells (gpu.py:56-67, 185-187) ----
     float* go = P.grad_per_slot ? P.grad + static_cast<size_t>(slot) * P.nz * P.nx
                                 : P.grad + static_cast<size_t>(solve) * P.nz * P.nx;
@@ -573,9 +236,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           for (int jj = P.pad + P.nx; jj < xhi; ++jj) val += G(i, jj);
         go[o] = val;
       }
-      const int warp = tid >> 5, lane = tid & 31;
-      if (rank == 0 && warp < 4) {
-        const int z = (warp & 1) ? P.nz - 1 : 0, x = (warp & 2) ? P.nx - 1 : 0;
+      const int warp = tid >> 5, lane = tid & 31, n_warps = nthr >> 5;
+      for (int corner = warp; rank == 0 && corner < 4; corner += n_warps) {
+        const int z = (corner & 1) ? P.nz - 1 : 0, x = (corner & 2) ? P.nx - 1 : 0;
         const int i = P.pad + z, j = P.pad + x;
         const int i0 = z == 0 ? zlo : P.pad + P.nz, i1 = z == 0 ? P.pad : zhi;
         const int j0 = x == 0 ? xlo : P.pad + P.nx, j1 = x == 0 ? P.pad : xhi;
@@ -634,6 +297,466 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         for (int o = gthr; o < P.nz * P.nx; o += gstride) im[o] = pre[o];
       }
     }
+}
+
+// Negated 9-point stencil, -S, of the four cells of one row (S = 12 dx^2 x the
+// 4th-order Laplacian of gpu.py:33-37).  r0..r4 are the rows -2..+2 of the
+// thread's four columns; lf / rt are the two columns left / right of them.
+// Pairs (columns 0-1, 2-3) go through the packed FP32x2 pipe.
+__device__ __forceinline__ void neg_stencil(const float4& r0, const float4& r1, const float4& r2, const float4& r3,
+                                            const float4& r4, const float2& lf, const float2& rt, float2& lo,
+                                            float2& hi) {
+  const float2 zn_lo = __fadd2_rn(make_float2(r1.x, r1.y), make_float2(r3.x, r3.y));
+  const float2 zn_hi = __fadd2_rn(make_float2(r1.z, r1.w), make_float2(r3.z, r3.w));
+  const float2 zf_lo = __fadd2_rn(make_float2(r0.x, r0.y), make_float2(r4.x, r4.y));
+  const float2 zf_hi = __fadd2_rn(make_float2(r0.z, r0.w), make_float2(r4.z, r4.w));
+  const float2 xn_lo = make_float2(lf.y + r2.y, r2.x + r2.z);
+  const float2 xn_hi = make_float2(r2.y + r2.w, r2.z + rt.x);
+  const float2 xf_lo = make_float2(lf.x + r2.z, lf.y + r2.w);
+  const float2 xf_hi = make_float2(r2.x + rt.x, r2.y + rt.y);
+  const float2 m16 = make_float2(-16.f, -16.f), p60 = make_float2(60.f, 60.f);
+  lo = __ffma2_rn(p60, make_float2(r2.x, r2.y), __ffma2_rn(m16, __fadd2_rn(zn_lo, xn_lo), __fadd2_rn(zf_lo, xf_lo)));
+  hi = __ffma2_rn(p60, make_float2(r2.z, r2.w), __ffma2_rn(m16, __fadd2_rn(zn_hi, xn_hi), __fadd2_rn(zf_hi, xf_hi)));
+}
+
+// new = old2 + kappa*(old1 - old2) - nsig*(-S), for a pair of cells.
+__device__ __forceinline__ float2 leapfrog(float2 kap, float2 nsig, float2 old1, float2 old2, float2 sneg) {
+  const float2 d = __ffma2_rn(make_float2(-1.f, -1.f), old2, old1);
+  return __ffma2_rn(nsig, sneg, __ffma2_rn(kap, d, old2));
+}
+
+__device__ __forceinline__ void st_async_v4(uint32_t addr, float4 v, uint32_t bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(addr),
+               "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ float pick(const float4& v, int m) {
+  return m == 0 ? v.x : m == 1 ? v.y : m == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ void add_at(float4& v, int m, float a) {
+  if (m == 0) v.x += a;
+  else if (m == 1) v.y += a;
+  else if (m == 2) v.z += a;
+  else v.w += a;
+}
+
+// Body of one tile row k (a compile-time constant after unrolling) inside
+// solve_kernel's step; written once, expanded in two row orders.
+#define SS_TILE_ROW(k) \
+          const float4 rm2 = k >= 2 ? as4(O1[k - 2]) : (k == 0 ? h0 : h1); \
+          const float4 rm1 = k >= 1 ? as4(O1[k - 1]) : h1; \
+          const float4 rc = as4(O1[k]); \
+          const float4 rp1 = k + 1 < H ? as4(O1[k + 1]) : h2; \
+          const float4 rp2 = k + 2 < H ? as4(O1[k + 2]) : (k + 2 == H ? h2 : h3); \
+          const float2 lf = *reinterpret_cast<const float2*>(xc + (k + 2) * RS - 2); \
+          const float2 rt = *reinterpret_cast<const float2*>(xc + (k + 2) * RS + 4); \
+          float2 s_lo, s_hi; \
+          neg_stencil(rm2, rm1, rc, rp1, rp2, lf, rt, s_lo, s_hi); \
+          const float2 n_lo = leapfrog(kap[k][0], nsig[k][0], O1[k][0], O2[k][0], s_lo); \
+          const float2 n_hi = leapfrog(kap[k][1], nsig[k][1], O1[k][1], O2[k][1], s_hi); \
+          float4 nw = make_float4(n_lo.x, n_lo.y, n_hi.x, n_hi.y); \
+          if (fwd) { \
+            if (warp_src && k == src_k) add_at(nw, src_m, wt);  /* injection after damping (gpu.py:113-114) */ \
+          } else { \
+            if (warp_rec && k == rec_k) {  /* residual injection th += sigma*res (gpu.py:180) */ \
+              const float* rs = bi ? S.res[1] : S.res[0]; \
+              const int rr = col0 - P.pad; \
+              if (rr >= 0 && rr < P.nx) nw.x = fmaf(-nsig[k][0].x, rs[rr], nw.x); \
+              if (rr + 1 >= 0 && rr + 1 < P.nx) nw.y = fmaf(-nsig[k][0].y, rs[rr + 1], nw.y); \
+              if (rr + 2 >= 0 && rr + 2 < P.nx) nw.z = fmaf(-nsig[k][1].x, rs[rr + 2], nw.z); \
+              if (rr + 3 >= 0 && rr + 3 < P.nx) nw.w = fmaf(-nsig[k][1].y, rs[rr + 3], nw.w); \
+            } \
+            if (warp_src && k == src_k) src_acc = fmaf(pick(nw, src_m), wt, src_acc);  /* gpu.py:182 */ \
+          } \
+          if ((push_rows >> k) & 1u) { \
+            if (k < 2 && edge_up) \
+              st_async_v4(up_addr + (cur ^ 1) * field_bytes + 4u * (k * RS), nw, up_bar + 8u * (cur ^ 1)); \
+            if (k >= H - 2 && edge_dn) \
+              st_async_v4(dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * RS), nw, dn_bar + 8u * (cur ^ 1)); \
+          } \
+          O2[k][0] = make_float2(nw.x, nw.y); \
+          O2[k][1] = make_float2(nw.z, nw.w); \
+          *reinterpret_cast<float4*>(yc + k * RS) = nw; \
+          if (fwd) { \
+            if (ADJ) { \
+              *reinterpret_cast<float4*>(stg + k * P.sw) = make_float4(s_lo.x, s_lo.y, s_hi.x, s_hi.y); \
+              acc[k][0] = __ffma2_rn(s_lo, s_lo, acc[k][0]); \
+              acc[k][1] = __ffma2_rn(s_hi, s_hi, acc[k][1]); \
+            } \
+          } else { \
+            const float4 h = *reinterpret_cast<const float4*>(hl + k * P.sw); \
+            acc[k][0] = __ffma2_rn(O2[k][0], make_float2(h.x, h.y), acc[k][0]); \
+            acc[k][1] = __ffma2_rn(O2[k][1], make_float2(h.z, h.w), acc[k][1]); \
+          }
+
+// RS_CT: shared-memory row stride known at compile time (0 = take P.rs).
+//
+// Each thread owns an H x 4 tile of cells and keeps both of its time levels
+// (old1 = t, old2 = t-1) in registers; shared memory carries only what the
+// neighbouring tiles read (the full field of the current level, ping-pong
+// buffered).  The time loop is unrolled by two so that the two register
+// arrays swap roles without moves.
+template <int MODE, int RS_CT>
+__global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) {
+  constexpr int H = kRowsPerThread;
+  constexpr bool ADJ = MODE != SS_MODE_FORWARD;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int RS = RS_CT ? RS_CT : P.rs;
+
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int rank = static_cast<int>(cluster_rank());
+  const int slot = static_cast<int>(cluster_id());
+  const int n_slots = static_cast<int>(cluster_count());
+
+  // ---- shared-memory carve-up (identical in every CTA of the cluster) ----
+  Smem S;
+  const size_t field_floats = static_cast<size_t>(P.bh + 4) * RS;
+  {
+    const size_t stage = ADJ ? static_cast<size_t>(P.bh) * P.sw : 0;
+    float* base = reinterpret_cast<float*>(smem_raw);
+    S.f[0] = base;
+    S.f[1] = base + field_floats;
+    S.stg[0] = base + 2 * field_floats;
+    S.stg[1] = base + 2 * field_floats + stage;
+    S.wav = base + 2 * field_floats + 2 * stage;
+    S.red = S.wav + ((P.nt + 31) & ~31);
+    S.res[0] = S.red + 32;
+    S.res[1] = S.res[0] + P.nxs;
+    S.trc = S.res[1] + P.nxs;
+    S.bar = reinterpret_cast<uint64_t*>(S.trc + kTraceRing * P.nxs);   // [0,1] history copies, [2,3] halos
+  }
+  for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
+  if (tid == 0) {
+    for (int b = 0; b < 4; ++b) mbar_init(smem_u32(&S.bar[b]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const uint32_t hist_bar0 = smem_u32(&S.bar[0]);
+  const uint32_t halo_bar0 = smem_u32(&S.bar[2]);
+  uint32_t hist_phase = 0, halo_phase = 0;   // parity of the next wait, one bit per buffer
+
+  // ---- this thread's tile -------------------------------------------------
+  // Warp-aligned mapping: the first nseg*ncg_main threads cover column
+  // groups [0, ncg_main) with one tile row per warp; the remaining column
+  // groups of every tile row are packed after them.
+  const bool active = tid < P.nact;
+  const int ncg_main = (P.ncg / 32) * 32, ncg_rem = P.ncg - ncg_main;
+  int cg = 0, seg = 0;
+  if (active) {
+    if (tid < P.nseg * ncg_main) {
+      seg = tid / ncg_main;
+      cg = tid - seg * ncg_main;
+    } else {
+      const int u = tid - P.nseg * ncg_main;
+      seg = u / ncg_rem;
+      cg = ncg_main + (u - seg * ncg_rem);
+    }
+  }
+  const int row0 = 2 + rank * P.bh;               // first padded row of the band
+  const int myrow = row0 + seg * H;               // first padded row of this thread
+  const int col0 = 2 + 4 * cg;                    // first padded column
+  const int o0 = 4 * cg + 4;                      // shared-memory column offset of col0
+  const int lr0 = seg * H;                        // shared row of tile row -2
+  const int src_r = P.pad + P.src_row;            // padded row of sources and receivers
+  const int rec_rank = (src_r - 2) / P.bh;
+
+  // Halo exchange: the two edge rows of a band are pushed into the
+  // neighbour's halo rows with st.async, which counts the bytes on the
+  // neighbour's halo mbarrier of that buffer; readers of halo rows wait on it.
+  const bool edge_up = active && seg == 0 && rank > 0;
+  const bool edge_dn = active && seg == P.nseg - 1 && rank < P.C - 1;
+  const uint32_t field_bytes = static_cast<uint32_t>(field_floats * sizeof(float));
+  const uint32_t up_addr = edge_up ? mapa(smem_u32(S.f[0] + (P.bh + 2) * RS + o0), rank - 1) : 0u;
+  const uint32_t up_bar = edge_up ? mapa(halo_bar0, rank - 1) : 0u;
+  const uint32_t dn_addr = edge_dn ? mapa(smem_u32(S.f[0] + o0), rank + 1) : 0u;
+  const uint32_t dn_bar = edge_dn ? mapa(halo_bar0, rank + 1) : 0u;
+  const uint32_t halo_bytes = 32u * P.ncg * ((rank > 0 ? 1u : 0u) + (rank < P.C - 1 ? 1u : 0u));
+  const int rec_k = (active && src_r >= myrow && src_r < myrow + H) ? src_r - myrow : -1;
+  // A warp with any tile on the lower band edge computes its rows bottom-up,
+  // so that the rows pushed to the next band are ready early in the step;
+  // the order is uniform per warp (the tile is in registers, any order works).
+  const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
+
+  const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * P.sw * sizeof(float));
+  const size_t hist_slot = static_cast<size_t>(P.nt) * P.C * P.bh * P.sw;
+  float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * P.sw
+                               : nullptr;
+  const size_t hist_step = static_cast<size_t>(P.C) * P.bh * P.sw;
+
+  cluster_sync();   // barriers initialised and wavelet staged everywhere
+
+  for (int solve = slot; solve < P.n_solves; solve += n_slots) {
+    const int b = solve / P.n_shots;
+    const int s = solve - b * P.n_shots;
+    const float* v = P.vel + static_cast<size_t>(b) * P.nz * P.nx;
+    const int shot_col = P.shot_cols[s];
+    const int src_c = P.pad + shot_col;
+
+    // ---- per-cell coefficients ----------------------------------------
+    float2 kap[H][2], nsig[H][2], acc[H][2], A[H][2], B[H][2];
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      float kvs[4], svs[4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int r = myrow + k, c = col0 + m;
+        float kv = 0.f, sv = 0.f;
+        if (active && r < P.nzp - 2 && c < P.nxp - 2) {
+          const double dz = layer_depth(r, P.nzp, P.pad), dxl = layer_depth(c, P.nxp, P.pad);
+          const float Ad = static_cast<float>(1.0 / (1.0 + P.damp_k * (dz * dz + dxl * dxl)));
+          const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
+          const double vp = v[vz * P.nx + vx];
+          const float c2 = static_cast<float>(vp * vp * P.dtdx2);
+          kv = 2.f * Ad;
+          sv = -((c2 * Ad) / 12.f);
+        }
+        kvs[m] = kv;
+        svs[m] = sv;
+      }
+      kap[k][0] = make_float2(kvs[0], kvs[1]);
+      kap[k][1] = make_float2(kvs[2], kvs[3]);
+      nsig[k][0] = make_float2(svs[0], svs[1]);
+      nsig[k][1] = make_float2(svs[2], svs[3]);
+      acc[k][0] = acc[k][1] = A[k][0] = A[k][1] = B[k][0] = B[k][1] = make_float2(0.f, 0.f);
+    }
+    int src_k = -1, src_m = 0;
+    if (active && src_r >= myrow && src_r < myrow + H && src_c >= col0 && src_c < col0 + 4) {
+      src_k = src_r - myrow;
+      src_m = src_c - col0;
+    }
+    // rows of this thread with extra work: source, receivers, halo pushes
+    // Halo rows pushed inside the row loop.  Injections and the source term
+    // run behind warp-uniform branches: only warps holding such cells pay.
+    const unsigned edge_rows = (edge_up ? 3u : 0u) | (edge_dn ? 3u << (H - 2) : 0u);
+    const bool warp_src = __any_sync(0xffffffffu, src_k >= 0);
+    const bool warp_rec = __any_sync(0xffffffffu, rec_k >= 0);
+    const double v_src = v[P.src_row * P.nx + shot_col];
+    const float amp = static_cast<float>((v_src / P.amp_ref) * (v_src / P.amp_ref));
+
+    const int tstride = (MODE == SS_MODE_FORWARD) ? P.nx : P.nxs;
+    float src_acc = 0.f;   // sum_t th(source cell) * w[t]
+    int flushed = 0;       // receiver rows below this level are in global memory
+    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + static_cast<size_t>(solve) * P.nt * P.nx
+                                             : P.trace + static_cast<size_t>(slot) * P.nt * P.nxs;
+
+    // ---- zero both shared fields (own rows and halos) --------------------
+    for (size_t i = tid; i < field_floats / 2; i += nthr) {
+      reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
+      reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
+    }
+    cluster_sync();
+
+    // One leapfrog step of the tile.  O1 = own cells at level t (old1), O2 =
+    // own cells at t-1 (old2), overwritten with level t+1.  step = index in
+    // the loop (0-based), lvl = time index t, cur = step & 1.
+    // FWD: source injection, receivers, history of -S (images/gradient).
+    // !FWD (adjoint): residual injection, source term, gradient correlation.
+    auto tile_step = [&](float2(&O1)[H][2], float2(&O2)[H][2], const int step, const int lvl, const int cur,
+                         const bool fwd) {
+      const float* X = cur ? S.f[1] : S.f[0];
+      float* Y = cur ? S.f[0] : S.f[1];
+      const bool more = step + 1 < P.nt;
+      const int bi = lvl & 1;
+      if (tid == 0 && more) {
+        if (halo_bytes) mbar_expect_tx(halo_bar0 + 8u * (cur ^ 1), halo_bytes);
+        if (!fwd) {   // history slab (and residual row) of the next adjoint step
+          const int tn = lvl - 1, bn = tn & 1;
+          const uint32_t bar = hist_bar0 + 8u * bn;
+          const bool res_here = rank == rec_rank;
+          const uint32_t res_bytes = static_cast<uint32_t>(P.nxs * sizeof(float));
+          mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
+          bulk_load(smem_u32(bn ? S.stg[1] : S.stg[0]), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes,
+                    bar);
+          if (res_here)
+            bulk_load(smem_u32(bn ? S.res[1] : S.res[0]), trace + static_cast<size_t>(tn) * P.nxs, res_bytes, bar);
+        }
+      }
+      if (MODE == SS_MODE_FORWARD && fwd && P.ckpt != nullptr && lvl % P.ckpt_interval == 0 && active) {
+        float* ck = P.ckpt + ((static_cast<size_t>(solve) * P.n_ckpt + lvl / P.ckpt_interval) * 2) * P.nzp * P.nxp;
+#pragma unroll
+        for (int k = 0; k < H; ++k) {
+          const int r = myrow + k;
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const int c = col0 + m;
+            if (r < P.nzp - 2 && c < P.nxp - 2) {
+              const float2 o2 = O2[k][m >> 1], o1 = O1[k][m >> 1];
+              ck[static_cast<size_t>(r) * P.nxp + c] = (m & 1) ? o2.y : o2.x;
+              ck[static_cast<size_t>(P.nzp) * P.nxp + static_cast<size_t>(r) * P.nxp + c] = (m & 1) ? o1.y : o1.x;
+            }
+          }
+        }
+      }
+      if ((edge_up || edge_dn) && step > 0) {
+        mbar_wait_bounded(halo_bar0 + 8u * cur, (halo_phase >> cur) & 1u, P.err);
+        halo_phase ^= 1u << cur;
+      }
+      if (!fwd) {
+        mbar_wait_bounded(hist_bar0 + 8u * bi, (hist_phase >> bi) & 1u, P.err);
+        hist_phase ^= 1u << bi;
+      }
+      const unsigned push_rows = more ? edge_rows : 0u;
+      if (fwd && rank == rec_rank && step > 0) {
+        // receivers at every model column (gpu.py:134): the level recorded at
+        // the previous step is now the read-only field X
+        for (int r = tid; r < P.nx; r += nthr)
+          S.trc[((lvl - 1) % kTraceRing) * P.nxs + r] = X[(src_r - row0 + 2) * RS + P.pad + r + 2];
+      }
+      if (active) {
+        const float wt = fwd ? S.wav[lvl] * amp : S.wav[lvl];
+        const float* xc = X + lr0 * RS + o0;          // tile row -2
+        float* yc = Y + (lr0 + 2) * RS + o0;          // tile row 0
+        const float4 h0 = *reinterpret_cast<const float4*>(xc);
+        const float4 h1 = *reinterpret_cast<const float4*>(xc + RS);
+        const float4 h2 = *reinterpret_cast<const float4*>(xc + (H + 2) * RS);
+        const float4 h3 = *reinterpret_cast<const float4*>(xc + (H + 3) * RS);
+        float* stg = (fwd && ADJ) ? (bi ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg : nullptr;
+        const float* hl = fwd ? nullptr : (bi ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg;
+        auto as4 = [](const float2(&r)[2]) { return make_float4(r[0].x, r[0].y, r[1].x, r[1].y); };
+        // Threads on the lower band edge compute their bottom rows first, so
+        // that the halo push to the next band leaves early in the step.
+        if (rev_rows) {
+#pragma unroll
+          for (int i = 0; i < H; ++i) {
+            const int k = H - 1 - i;
+            SS_TILE_ROW(k)
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < H; ++k) {
+            SS_TILE_ROW(k)
+          }
+        }
+      }
+      if (fwd && ADJ) {
+        fence_proxy_async_smem();
+        if (tid == 0 && step > 0) bulk_wait_read_all();   // store of the previous step has left shared memory
+      }
+      __syncthreads();
+      if (fwd && ADJ && tid == 0)
+        bulk_store(hist_mine + static_cast<size_t>(lvl) * hist_step, smem_u32(bi ? S.stg[1] : S.stg[0]), stage_bytes);
+      if (fwd && rank == rec_rank) {
+        // The ring holds the receiver rows [flushed, lvl-1] (level lvl-1 was
+        // recorded at this step's start).  A full ring, and at the end every
+        // remaining row, goes to global memory, coalesced.
+        auto flush = [&](int hi) {
+          __syncthreads();
+          const int n = (hi - flushed + 1) * P.nx;
+          for (int i = tid; i < n; i += nthr) {
+            const int tt = flushed + i / P.nx, r = i % P.nx;
+            trace[static_cast<size_t>(tt) * tstride + r] = S.trc[(tt % kTraceRing) * P.nxs + r];
+          }
+          __syncthreads();
+          flushed = hi + 1;
+        };
+        if (lvl - flushed == kTraceRing) flush(lvl - 1);
+        if (lvl == P.nt - 1) {   // the last level, recorded after the final barrier
+          for (int r = tid; r < P.nx; r += nthr)
+            S.trc[(lvl % kTraceRing) * P.nxs + r] = Y[(src_r - row0 + 2) * RS + P.pad + r + 2];
+          flush(lvl);
+        }
+      }
+    };
+
+    // ================= forward: t = 0 .. nt-1 =============================
+    {
+      int t = 0;
+      for (; t + 1 < P.nt; t += 2) {
+        tile_step(A, B, t, t, 0, true);
+        tile_step(B, A, t + 1, t + 1, 1, true);
+      }
+      if (t < P.nt) tile_step(A, B, t, t, 0, true);
+    }
+
+    if (MODE == SS_MODE_FORWARD) continue;
+
+    // ---- forward epilogue: illumination = sum_t (S/12)^2 on model cells --
+    if (tid == 0) {
+      bulk_wait_all();
+      fence_proxy_async_all();
+    }
+    {
+      float* il = P.illum + static_cast<size_t>(solve) * P.nz * P.nx;
+#pragma unroll
+      for (int k = 0; k < H; ++k)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int z = myrow + k - P.pad, x = col0 + m - P.pad;
+          const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
+          if (active && z >= 0 && z < P.nz && x >= 0 && x < P.nx) il[z * P.nx + x] = a * (1.f / 144.f);
+        }
+#pragma unroll
+      for (int k = 0; k < H; ++k)
+        acc[k][0] = acc[k][1] = A[k][0] = A[k][1] = B[k][0] = B[k][1] = make_float2(0.f, 0.f);
+    }
+    // ---- residual (sim - obs) * mute, in place over the trace ------------
+    if (rank == rec_rank) {
+      const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * P.nx;
+      const float vm = P.vmute ? P.vmute[b] : 0.f;
+      for (int i = tid; i < P.nt * P.nx; i += nthr) {
+        const int t = i / P.nx, r = i - t * P.nx;
+        const float o = ob[i];
+        if (!isfinite(o)) atomicExch(P.err, static_cast<int>(SS_ERR_NONFINITE));
+        float res = trace[t * P.nxs + r] - o;
+        if (P.vmute) res *= mute_weight(t, r, shot_col, P.dx, P.dt, vm, P.t_mute);
+        trace[t * P.nxs + r] = res;
+      }
+      fence_proxy_async_all();   // these rows are read back by bulk copies
+      __syncthreads();
+    }
+
+    // ================= adjoint: t = nt-1 .. 0 =============================
+    for (size_t i = tid; i < field_floats / 2; i += nthr) {
+      reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
+      reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
+    }
+    cluster_sync();
+    if (tid == 0) {   // history slab and residual row of the first adjoint step
+      const int tn = P.nt - 1, bn = tn & 1;
+      const uint32_t bar = hist_bar0 + 8u * bn;
+      const bool res_here = rank == rec_rank;
+      const uint32_t res_bytes = static_cast<uint32_t>(P.nxs * sizeof(float));
+      mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
+      bulk_load(smem_u32(bn ? S.stg[1] : S.stg[0]), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes, bar);
+      if (res_here)
+        bulk_load(smem_u32(bn ? S.res[1] : S.res[0]), trace + static_cast<size_t>(tn) * P.nxs, res_bytes, bar);
+    }
+    {
+      int i = 0;
+      for (; i + 1 < P.nt; i += 2) {
+        tile_step(A, B, i, P.nt - 1 - i, 0, false);
+        tile_step(B, A, i + 1, P.nt - 2 - i, 1, false);
+      }
+      if (i < P.nt) tile_step(A, B, i, P.nt - 1 - i, 0, false);
+    }
+
+    // ---- padded gradient 2/v * sum_t th*S(p), plus the source term -------
+    // acc holds -sum_t th*S (the history holds -S); nsig = -sigma.
+    float* gp = P.gpad + static_cast<size_t>(slot) * P.nzp * P.nxp;
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < H; ++k)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int r = myrow + k, c = col0 + m;
+          if (r < P.nzp - 2 && c < P.nxp - 2) {
+            const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
+            const float vp = v[vz * P.nx + vx];
+            const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
+            float gval = -2.f * a / vp;
+            if (k == src_k && m == src_m) {
+              const float deriv = static_cast<float>(2.0 * v_src / (P.amp_ref * P.amp_ref));
+              const float ns = (m & 1) ? nsig[k][m >> 1].y : nsig[k][m >> 1].x;
+              gval += src_acc * deriv / -ns;
+            }
+            gp[static_cast<size_t>(r) * P.nxp + c] = gval;
+          }
+        }
+    }
+    __threadfence();
+    cluster_sync();
+    epilogue<MODE>(P, S, gp, solve, slot, rank, tid, nthr);
     __threadfence();
     cluster_sync();   // scratch of this slot is free for the next solve
   }
@@ -759,19 +882,24 @@ int check_geometry(const ss_geometry* g) {
   return SS_OK;
 }
 
-const void* kernel_for(int mode) {
+using SolveFn = void (*)(KParams);
+constexpr int kFastRS = 156;   // row stride of the 150-column padded OpenFWI grid (37 column groups)
+
+SolveFn kernel_for(int mode, int rs) {
+  const bool fast = rs == kFastRS;
   switch (mode) {
-    case SS_MODE_FORWARD: return reinterpret_cast<const void*>(&solve_kernel<SS_MODE_FORWARD>);
-    case SS_MODE_GRADIENT: return reinterpret_cast<const void*>(&solve_kernel<SS_MODE_GRADIENT>);
-    default: return reinterpret_cast<const void*>(&solve_kernel<SS_MODE_IMAGES>);
+    case SS_MODE_FORWARD: return fast ? solve_kernel<SS_MODE_FORWARD, kFastRS> : solve_kernel<SS_MODE_FORWARD, 0>;
+    case SS_MODE_GRADIENT: return fast ? solve_kernel<SS_MODE_GRADIENT, kFastRS> : solve_kernel<SS_MODE_GRADIENT, 0>;
+    default: return fast ? solve_kernel<SS_MODE_IMAGES, kFastRS> : solve_kernel<SS_MODE_IMAGES, 0>;
   }
 }
 
 size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj) {
   const size_t field = static_cast<size_t>(bh + 4) * rs;
   const size_t stage = adj ? static_cast<size_t>(bh) * sw : 0;
-  return (2 * field + 2 * stage + ((nt + 31) & ~31) + 32 + 2 * static_cast<size_t>(nxs)) * sizeof(float) +
-         2 * sizeof(uint64_t);
+  return (2 * field + 2 * stage + ((nt + 31) & ~31) + 32 + (2 + kTraceRing) * static_cast<size_t>(nxs)) *
+             sizeof(float) +
+         4 * sizeof(uint64_t);
 }
 
 int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
@@ -803,7 +931,7 @@ int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
   }
   if (!ok) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits shared memory for this grid");
   p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
-  const void* fn = kernel_for(mode);
+  const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->rs));
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->smem));
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   if (p->C > 8) {
@@ -897,12 +1025,7 @@ int launch(const Plan& p, int mode, const KParams& k, cudaStream_t stream) {
   cfg.stream = stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t e;
-  switch (mode) {
-    case SS_MODE_FORWARD: e = cudaLaunchKernelEx(&cfg, solve_kernel<SS_MODE_FORWARD>, k); break;
-    case SS_MODE_GRADIENT: e = cudaLaunchKernelEx(&cfg, solve_kernel<SS_MODE_GRADIENT>, k); break;
-    default: e = cudaLaunchKernelEx(&cfg, solve_kernel<SS_MODE_IMAGES>, k); break;
-  }
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel_for(mode, p.rs), k);
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaLaunchKernelEx: ") + cudaGetErrorString(e));
   return SS_OK;
 }

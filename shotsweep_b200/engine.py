@@ -28,6 +28,8 @@ class Engine:
         self.g = geom
         self.device = torch.device('cuda') if device is None else torch.device(device)
         _lib.require_cuda(self.device)
+        if self.device.index is None:
+            self.device = torch.device('cuda', torch.cuda.current_device())
         self.L = _lib.load()
         self._ws = None
 

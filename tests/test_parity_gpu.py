@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 
 GATHER_TOL = 1e-5
 IMAGE_TOL = 2e-4
+FIELD_TOL = 5e-5     # whole padded wavefields (checkpoints), which include the weak far field
 
 
 def rel(a, b):
@@ -95,7 +96,7 @@ def test_forward_returns_reference_structures(gpu, plain):
     o_out, o_ck, o_c2 = osim.forward(plain['model'][None].astype(np.float64), store=True)
     for it in (250, 750):
         for j in (0, 1):
-            assert rel(ck[it][j].cpu().numpy(), o_ck[it][j].numpy()) <= GATHER_TOL
+            assert rel(ck[it][j].cpu().numpy(), o_ck[it][j].numpy()) <= FIELD_TOL
     assert rel(c2.cpu().numpy(), o_c2.numpy()) <= 1e-6
 
 
@@ -155,7 +156,8 @@ def test_odd_geometries_match_oracle(case):
     osim = O.OracleSim(wavelet=wav, pad=pad, geom=geom, checkpoint_interval=17)
     obs = osim.gathers(truth)
     vm = np.array([1800.0, 2100.0])
-    o_grad, o_illum = osim.gradient(bg, obs, v_mute=vm)
+    t_mute = 0.02 * nt * 1e-3          # short records: mute only the first fifth
+    o_grad, o_illum = osim.gradient(bg, obs, v_mute=vm, t_mute=t_mute)
     o_img = O.image_epilogue(torch.from_numpy(o_grad), torch.from_numpy(o_illum)).numpy()
 
     eng = engine.Engine(engine.geometry(nz, nx, nt, pad, cols, src_row))
@@ -166,10 +168,14 @@ def test_odd_geometries_match_oracle(case):
     v = torch.tensor(bg, dtype=torch.float32, device=dev)
     ob = torch.tensor(obs, dtype=torch.float32, device=dev)
     vmd = torch.tensor(vm, dtype=torch.float32, device=dev)
-    grad, illum = eng.gradient(v, w, ob, vmd)
+    grad, illum = eng.gradient(v, w, ob, vmd, t_mute)
     eng.status()
     assert per_image_rel(grad.cpu().numpy(), o_grad).max() <= IMAGE_TOL
     assert per_image_rel(illum.cpu().numpy(), o_illum).max() <= IMAGE_TOL
-    img, illum2, grad2 = eng.images(v, w, ob, vmd, want_grad=True)
+    img, illum2, grad2 = eng.images(v, w, ob, vmd, t_mute, want_grad=True)
     assert per_image_rel(img.cpu().numpy(), o_img).max() <= IMAGE_TOL
     np.testing.assert_array_equal(grad2.cpu().numpy(), grad.cpu().numpy())
+    # no mute at all
+    o_grad0, _ = osim.gradient(bg, obs)
+    grad0, _ = eng.gradient(v, w, ob)
+    assert per_image_rel(grad0.cpu().numpy(), o_grad0).max() <= IMAGE_TOL
