@@ -43,6 +43,8 @@ constexpr int kRowsPerThread = 5;          // H: rows per thread in the band
 constexpr int kMaxThreads = 384;           // register budget: 168 regs/thread
 constexpr int kMaxCluster = 16;
 constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush
+constexpr int kStages = 3;                 // history slabs in flight: prefetch / retire depth kStages-1
+constexpr int kFastRS = 156;               // shared row stride of the 150-column padded OpenFWI grid
 constexpr size_t kMaxSmem = 227 * 1024;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s per bounded wait
 
@@ -137,6 +139,11 @@ __device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t byt
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// At most kStages-2 newer history stores may still be reading shared memory.
+__device__ __forceinline__ void bulk_wait_read_lag() {
+  static_assert(kStages == 3, "the immediate below is kStages - 2");
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -190,11 +197,12 @@ struct KParams {
 
 struct Smem {
   float* f[2];
-  float* stg[2];
+  float* stg0;     // kStages history slabs of bh x sw, consecutive
   float* wav;
   float* red;
-  float* res[2];   // residual row of the current / next adjoint step
+  float* res0;     // kStages residual rows of nxs, consecutive
   float* trc;      // ring of kTraceRing receiver rows, flushed to global memory
+  float* dummy;    // zero tile for lanes without cells: (H + 4) rows of RS, then H rows of sw
   uint64_t* bar;
 };
 
@@ -325,6 +333,15 @@ __device__ __forceinline__ float2 leapfrog(float2 kap, float2 nsig, float2 old1,
   return __ffma2_rn(nsig, sneg, __ffma2_rn(kap, d, old2));
 }
 
+// Predicated form: no branch (and no divergence bookkeeping) in the row loop.
+__device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, uint32_t bar) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %6, 0;\n\t"
+      "@q st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];\n\t}" ::"r"(addr),
+      "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(bar), "r"(static_cast<uint32_t>(p))
+      : "memory");
+}
+
 __device__ __forceinline__ void st_async_v4(uint32_t addr, float4 v, uint32_t bar) {
   asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(addr),
                "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(bar)
@@ -357,84 +374,107 @@ __device__ __forceinline__ void add_at(float4& v, int m, float a) {
           const float2 n_hi = leapfrog(kap[k][1], nsig[k][1], O1[k][1], O2[k][1], s_hi); \
           float4 nw = make_float4(n_lo.x, n_lo.y, n_hi.x, n_hi.y); \
           if (fwd) { \
-            if (warp_src && k == src_k) add_at(nw, src_m, wt);  /* injection after damping (gpu.py:113-114) */ \
-          } else { \
-            if (warp_rec && k == rec_k) {  /* residual injection th += sigma*res (gpu.py:180) */ \
-              const float* rs = bi ? S.res[1] : S.res[0]; \
-              const int rr = col0 - P.pad; \
-              if (rr >= 0 && rr < P.nx) nw.x = fmaf(-nsig[k][0].x, rs[rr], nw.x); \
-              if (rr + 1 >= 0 && rr + 1 < P.nx) nw.y = fmaf(-nsig[k][0].y, rs[rr + 1], nw.y); \
-              if (rr + 2 >= 0 && rr + 2 < P.nx) nw.z = fmaf(-nsig[k][1].x, rs[rr + 2], nw.z); \
-              if (rr + 3 >= 0 && rr + 3 < P.nx) nw.w = fmaf(-nsig[k][1].y, rs[rr + 3], nw.w); \
+            if (warp_src) {  /* injection after damping (gpu.py:113-114) */ \
+              const float a = (k == src_k) ? wt : 0.f; \
+              nw.x += (src_m == 0) ? a : 0.f; \
+              nw.y += (src_m == 1) ? a : 0.f; \
+              nw.z += (src_m == 2) ? a : 0.f; \
+              nw.w += (src_m == 3) ? a : 0.f; \
             } \
-            if (warp_src && k == src_k) src_acc = fmaf(pick(nw, src_m), wt, src_acc);  /* gpu.py:182 */ \
+          } else { \
+            if (warp_rec) {  /* residual injection th += sigma*res (gpu.py:180) */ \
+              const float* rs = res_buf(bi); \
+              const int rr = col0 - PAD; \
+              const bool on = k == rec_k; \
+              const float r0v = rs[min(max(rr, 0), NX - 1)], r1v = rs[min(max(rr + 1, 0), NX - 1)]; \
+              const float r2v = rs[min(max(rr + 2, 0), NX - 1)], r3v = rs[min(max(rr + 3, 0), NX - 1)]; \
+              nw.x = fmaf((on && rr >= 0 && rr < NX) ? -nsig[k][0].x : 0.f, r0v, nw.x); \
+              nw.y = fmaf((on && rr + 1 >= 0 && rr + 1 < NX) ? -nsig[k][0].y : 0.f, r1v, nw.y); \
+              nw.z = fmaf((on && rr + 2 >= 0 && rr + 2 < NX) ? -nsig[k][1].x : 0.f, r2v, nw.z); \
+              nw.w = fmaf((on && rr + 3 >= 0 && rr + 3 < NX) ? -nsig[k][1].y : 0.f, r3v, nw.w); \
+            } \
+            if (warp_src) {  /* source-strength term (gpu.py:182) */ \
+              const float a = (k == src_k) ? wt : 0.f; \
+              const float q = src_m == 0 ? nw.x : src_m == 1 ? nw.y : src_m == 2 ? nw.z : nw.w; \
+              src_acc = fmaf(q, a, src_acc); \
+            } \
           } \
-          if ((push_rows >> k) & 1u) { \
-            if (k < 2 && edge_up) \
-              st_async_v4(up_addr + (cur ^ 1) * field_bytes + 4u * (k * RS), nw, up_bar + 8u * (cur ^ 1)); \
-            if (k >= H - 2 && edge_dn) \
-              st_async_v4(dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * RS), nw, dn_bar + 8u * (cur ^ 1)); \
-          } \
+          if (k < 2) \
+            st_async_v4_if(push_up, up_addr + (cur ^ 1) * field_bytes + 4u * (k * RS), nw, up_bar + 8u * (cur ^ 1)); \
+          if (k >= H - 2) \
+            st_async_v4_if(push_dn, dn_addr + (cur ^ 1) * field_bytes + 4u * ((k - (H - 2)) * RS), nw, \
+                           dn_bar + 8u * (cur ^ 1)); \
           O2[k][0] = make_float2(nw.x, nw.y); \
           O2[k][1] = make_float2(nw.z, nw.w); \
           *reinterpret_cast<float4*>(yc + k * RS) = nw; \
           if (fwd) { \
             if (ADJ) { \
-              *reinterpret_cast<float4*>(stg + k * P.sw) = make_float4(s_lo.x, s_lo.y, s_hi.x, s_hi.y); \
+              *reinterpret_cast<float4*>(stg + k * SW) = make_float4(s_lo.x, s_lo.y, s_hi.x, s_hi.y); \
               acc[k][0] = __ffma2_rn(s_lo, s_lo, acc[k][0]); \
               acc[k][1] = __ffma2_rn(s_hi, s_hi, acc[k][1]); \
             } \
           } else { \
-            const float4 h = *reinterpret_cast<const float4*>(hl + k * P.sw); \
+            const float4 h = *reinterpret_cast<const float4*>(hl + k * SW); \
             acc[k][0] = __ffma2_rn(O2[k][0], make_float2(h.x, h.y), acc[k][0]); \
             acc[k][1] = __ffma2_rn(O2[k][1], make_float2(h.z, h.w), acc[k][1]); \
           }
 
-// RS_CT: shared-memory row stride known at compile time (0 = take P.rs).
+// FAST: the OpenFWI geometry (nx = 70, pad = 40), whose strides are
+// compile-time constants; otherwise they come from the parameters.
 //
 // Each thread owns an H x 4 tile of cells and keeps both of its time levels
 // (old1 = t, old2 = t-1) in registers; shared memory carries only what the
 // neighbouring tiles read (the full field of the current level, ping-pong
 // buffered).  The time loop is unrolled by two so that the two register
 // arrays swap roles without moves.
-template <int MODE, int RS_CT>
+template <int MODE, bool FAST>
 __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) {
   constexpr int H = kRowsPerThread;
   constexpr bool ADJ = MODE != SS_MODE_FORWARD;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int RS = RS_CT ? RS_CT : P.rs;
+  // Geometry: compile-time constants on the fast path, parameter-bank reads
+  // otherwise (macros, so that the generic path keeps no registers for them).
+#define RS (FAST ? kFastRS : P.rs)      /* shared row stride (floats) */
+#define NX (FAST ? 70 : P.nx)           /* receivers per shot */
+#define PAD (FAST ? 40 : P.pad)
+#define SW (FAST ? kFastRS - 8 : P.sw)  /* history row width */
+#define NXS (FAST ? 72 : P.nxs)         /* padded trace row */
 
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
-  const int rank = static_cast<int>(cluster_rank());
-  const int slot = static_cast<int>(cluster_id());
-  const int n_slots = static_cast<int>(cluster_count());
+  // A 1-D grid of 1-D clusters: the CTA's rank in its cluster and the
+  // cluster index follow from blockIdx, which the compiler knows is uniform.
+  const int rank = static_cast<int>(blockIdx.x % P.C);
+  const int slot = static_cast<int>(blockIdx.x / P.C);
+  const int n_slots = static_cast<int>(gridDim.x / P.C);
 
   // ---- shared-memory carve-up (identical in every CTA of the cluster) ----
   Smem S;
   const size_t field_floats = static_cast<size_t>(P.bh + 4) * RS;
   {
-    const size_t stage = ADJ ? static_cast<size_t>(P.bh) * P.sw : 0;
+    const size_t stage = ADJ ? static_cast<size_t>(P.bh) * SW : 0;
     float* base = reinterpret_cast<float*>(smem_raw);
     S.f[0] = base;
     S.f[1] = base + field_floats;
-    S.stg[0] = base + 2 * field_floats;
-    S.stg[1] = base + 2 * field_floats + stage;
-    S.wav = base + 2 * field_floats + 2 * stage;
+    S.stg0 = base + 2 * field_floats;
+    S.wav = base + 2 * field_floats + kStages * stage;
     S.red = S.wav + ((P.nt + 31) & ~31);
-    S.res[0] = S.red + 32;
-    S.res[1] = S.res[0] + P.nxs;
-    S.trc = S.res[1] + P.nxs;
-    S.bar = reinterpret_cast<uint64_t*>(S.trc + kTraceRing * P.nxs);   // [0,1] history copies, [2,3] halos
+    S.res0 = S.red + 32;
+    S.trc = S.res0 + kStages * NXS;
+    S.dummy = S.trc + kTraceRing * NXS;
+    S.bar = reinterpret_cast<uint64_t*>(S.dummy + (H + 4) * RS + H * SW);   // [0,kStages) history, then 2 halos
   }
   for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
   if (tid == 0) {
-    for (int b = 0; b < 4; ++b) mbar_init(smem_u32(&S.bar[b]), 1);
+    for (int b = 0; b < kStages + 2; ++b) mbar_init(smem_u32(&S.bar[b]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   const uint32_t hist_bar0 = smem_u32(&S.bar[0]);
-  const uint32_t halo_bar0 = smem_u32(&S.bar[2]);
+  const uint32_t halo_bar0 = smem_u32(&S.bar[kStages]);
+  const size_t stage_floats = ADJ ? static_cast<size_t>(P.bh) * SW : 0;
   uint32_t hist_phase = 0, halo_phase = 0;   // parity of the next wait, one bit per buffer
+  auto stage_buf = [&](int b) { return S.stg0 + b * stage_floats; };
+  auto res_buf = [&](int b) { return S.res0 + b * NXS; };
 
   // ---- this thread's tile -------------------------------------------------
   // Warp-aligned mapping: the first nseg*ncg_main threads cover column
@@ -458,7 +498,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   const int col0 = 2 + 4 * cg;                    // first padded column
   const int o0 = 4 * cg + 4;                      // shared-memory column offset of col0
   const int lr0 = seg * H;                        // shared row of tile row -2
-  const int src_r = P.pad + P.src_row;            // padded row of sources and receivers
+  const int src_r = PAD + P.src_row;            // padded row of sources and receivers
   const int rec_rank = (src_r - 2) / P.bh;
 
   // Halo exchange: the two edge rows of a band are pushed into the
@@ -478,20 +518,20 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   // the order is uniform per warp (the tile is in registers, any order works).
   const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
 
-  const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * P.sw * sizeof(float));
-  const size_t hist_slot = static_cast<size_t>(P.nt) * P.C * P.bh * P.sw;
-  float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * P.sw
+  const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * SW * sizeof(float));
+  const size_t hist_slot = static_cast<size_t>(P.nt) * P.C * P.bh * SW;
+  float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * SW
                                : nullptr;
-  const size_t hist_step = static_cast<size_t>(P.C) * P.bh * P.sw;
+  const size_t hist_step = static_cast<size_t>(P.C) * P.bh * SW;
 
   cluster_sync();   // barriers initialised and wavelet staged everywhere
 
   for (int solve = slot; solve < P.n_solves; solve += n_slots) {
     const int b = solve / P.n_shots;
     const int s = solve - b * P.n_shots;
-    const float* v = P.vel + static_cast<size_t>(b) * P.nz * P.nx;
+    const float* v = P.vel + static_cast<size_t>(b) * P.nz * NX;
     const int shot_col = P.shot_cols[s];
-    const int src_c = P.pad + shot_col;
+    const int src_c = PAD + shot_col;
 
     // ---- per-cell coefficients ----------------------------------------
     float2 kap[H][2], nsig[H][2], acc[H][2], A[H][2], B[H][2];
@@ -503,10 +543,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         const int r = myrow + k, c = col0 + m;
         float kv = 0.f, sv = 0.f;
         if (active && r < P.nzp - 2 && c < P.nxp - 2) {
-          const double dz = layer_depth(r, P.nzp, P.pad), dxl = layer_depth(c, P.nxp, P.pad);
+          const double dz = layer_depth(r, P.nzp, PAD), dxl = layer_depth(c, P.nxp, PAD);
           const float Ad = static_cast<float>(1.0 / (1.0 + P.damp_k * (dz * dz + dxl * dxl)));
-          const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
-          const double vp = v[vz * P.nx + vx];
+          const int vz = min(max(r - PAD, 0), P.nz - 1), vx = min(max(c - PAD, 0), NX - 1);
+          const double vp = v[vz * NX + vx];
           const float c2 = static_cast<float>(vp * vp * P.dtdx2);
           kv = 2.f * Ad;
           sv = -((c2 * Ad) / 12.f);
@@ -528,23 +568,24 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     // rows of this thread with extra work: source, receivers, halo pushes
     // Halo rows pushed inside the row loop.  Injections and the source term
     // run behind warp-uniform branches: only warps holding such cells pay.
-    const unsigned edge_rows = (edge_up ? 3u : 0u) | (edge_dn ? 3u << (H - 2) : 0u);
     const bool warp_src = __any_sync(0xffffffffu, src_k >= 0);
     const bool warp_rec = __any_sync(0xffffffffu, rec_k >= 0);
-    const double v_src = v[P.src_row * P.nx + shot_col];
+    const double v_src = v[P.src_row * NX + shot_col];
     const float amp = static_cast<float>((v_src / P.amp_ref) * (v_src / P.amp_ref));
 
-    const int tstride = (MODE == SS_MODE_FORWARD) ? P.nx : P.nxs;
+    const int tstride = (MODE == SS_MODE_FORWARD) ? NX : NXS;
     float src_acc = 0.f;   // sum_t th(source cell) * w[t]
     int flushed = 0;       // receiver rows below this level are in global memory
-    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + static_cast<size_t>(solve) * P.nt * P.nx
-                                             : P.trace + static_cast<size_t>(slot) * P.nt * P.nxs;
+    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + static_cast<size_t>(solve) * P.nt * NX
+                                             : P.trace + static_cast<size_t>(slot) * P.nt * NXS;
 
     // ---- zero both shared fields (own rows and halos) --------------------
     for (size_t i = tid; i < field_floats / 2; i += nthr) {
       reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
       reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
     }
+    #pragma unroll 1
+    for (int i = tid; i < (H + 4) * RS + H * SW; i += nthr) S.dummy[i] = 0.f;
     cluster_sync();
 
     // One leapfrog step of the tile.  O1 = own cells at level t (old1), O2 =
@@ -557,19 +598,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       const float* X = cur ? S.f[1] : S.f[0];
       float* Y = cur ? S.f[0] : S.f[1];
       const bool more = step + 1 < P.nt;
-      const int bi = lvl & 1;
+      const int bi = lvl % kStages;
       if (tid == 0 && more) {
         if (halo_bytes) mbar_expect_tx(halo_bar0 + 8u * (cur ^ 1), halo_bytes);
-        if (!fwd) {   // history slab (and residual row) of the next adjoint step
-          const int tn = lvl - 1, bn = tn & 1;
+        if (!fwd && lvl - (kStages - 1) >= 0) {   // history slab (and residual row) kStages-1 steps ahead
+          const int tn = lvl - (kStages - 1), bn = tn % kStages;
           const uint32_t bar = hist_bar0 + 8u * bn;
           const bool res_here = rank == rec_rank;
-          const uint32_t res_bytes = static_cast<uint32_t>(P.nxs * sizeof(float));
+          const uint32_t res_bytes = static_cast<uint32_t>(NXS * sizeof(float));
           mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
-          bulk_load(smem_u32(bn ? S.stg[1] : S.stg[0]), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes,
-                    bar);
-          if (res_here)
-            bulk_load(smem_u32(bn ? S.res[1] : S.res[0]), trace + static_cast<size_t>(tn) * P.nxs, res_bytes, bar);
+          bulk_load(smem_u32(stage_buf(bn)), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes, bar);
+          if (res_here) bulk_load(smem_u32(res_buf(bn)), trace + static_cast<size_t>(tn) * NXS, res_bytes, bar);
         }
       }
       if (MODE == SS_MODE_FORWARD && fwd && P.ckpt != nullptr && lvl % P.ckpt_interval == 0 && active) {
@@ -596,23 +635,27 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         mbar_wait_bounded(hist_bar0 + 8u * bi, (hist_phase >> bi) & 1u, P.err);
         hist_phase ^= 1u << bi;
       }
-      const unsigned push_rows = more ? edge_rows : 0u;
+      const bool push_up = more && edge_up, push_dn = more && edge_dn;
       if (fwd && rank == rec_rank && step > 0) {
         // receivers at every model column (gpu.py:134): the level recorded at
         // the previous step is now the read-only field X
-        for (int r = tid; r < P.nx; r += nthr)
-          S.trc[((lvl - 1) % kTraceRing) * P.nxs + r] = X[(src_r - row0 + 2) * RS + P.pad + r + 2];
+        #pragma unroll 1
+        for (int r = tid; r < NX; r += nthr)
+          S.trc[((lvl - 1) % kTraceRing) * NXS + r] = X[(src_r - row0 + 2) * RS + PAD + r + 2];
       }
-      if (active) {
+      {
+        // Lanes without a tile run the same code on a private zero tile
+        // (zero coefficients keep it zero), so the loop needs no branch.
         const float wt = fwd ? S.wav[lvl] * amp : S.wav[lvl];
-        const float* xc = X + lr0 * RS + o0;          // tile row -2
-        float* yc = Y + (lr0 + 2) * RS + o0;          // tile row 0
+        const float* xc = active ? X + lr0 * RS + o0 : S.dummy;      // tile row -2
+        float* yc = active ? Y + (lr0 + 2) * RS + o0 : S.dummy + 2 * RS;   // tile row 0
         const float4 h0 = *reinterpret_cast<const float4*>(xc);
         const float4 h1 = *reinterpret_cast<const float4*>(xc + RS);
         const float4 h2 = *reinterpret_cast<const float4*>(xc + (H + 2) * RS);
         const float4 h3 = *reinterpret_cast<const float4*>(xc + (H + 3) * RS);
-        float* stg = (fwd && ADJ) ? (bi ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg : nullptr;
-        const float* hl = fwd ? nullptr : (bi ? S.stg[1] : S.stg[0]) + lr0 * P.sw + 4 * cg;
+        float* const dstg = S.dummy + (H + 4) * RS;
+        float* stg = (fwd && ADJ) ? (active ? stage_buf(bi) + lr0 * SW + 4 * cg : dstg) : nullptr;
+        const float* hl = fwd ? nullptr : (active ? stage_buf(bi) + lr0 * SW + 4 * cg : dstg);
         auto as4 = [](const float2(&r)[2]) { return make_float4(r[0].x, r[0].y, r[1].x, r[1].y); };
         // Threads on the lower band edge compute their bottom rows first, so
         // that the halo push to the next band leaves early in the step.
@@ -631,29 +674,31 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       }
       if (fwd && ADJ) {
         fence_proxy_async_smem();
-        if (tid == 0 && step > 0) bulk_wait_read_all();   // store of the previous step has left shared memory
+        if (tid == 0 && step > 0) bulk_wait_read_lag();   // the slab to be refilled next step has left shared memory
       }
       __syncthreads();
       if (fwd && ADJ && tid == 0)
-        bulk_store(hist_mine + static_cast<size_t>(lvl) * hist_step, smem_u32(bi ? S.stg[1] : S.stg[0]), stage_bytes);
+        bulk_store(hist_mine + static_cast<size_t>(lvl) * hist_step, smem_u32(stage_buf(bi)), stage_bytes);
       if (fwd && rank == rec_rank) {
         // The ring holds the receiver rows [flushed, lvl-1] (level lvl-1 was
         // recorded at this step's start).  A full ring, and at the end every
         // remaining row, goes to global memory, coalesced.
         auto flush = [&](int hi) {
           __syncthreads();
-          const int n = (hi - flushed + 1) * P.nx;
+          const int n = (hi - flushed + 1) * NX;
+          #pragma unroll 1
           for (int i = tid; i < n; i += nthr) {
-            const int tt = flushed + i / P.nx, r = i % P.nx;
-            trace[static_cast<size_t>(tt) * tstride + r] = S.trc[(tt % kTraceRing) * P.nxs + r];
+            const int tt = flushed + i / NX, r = i % NX;
+            trace[static_cast<size_t>(tt) * tstride + r] = S.trc[(tt % kTraceRing) * NXS + r];
           }
           __syncthreads();
           flushed = hi + 1;
         };
         if (lvl - flushed == kTraceRing) flush(lvl - 1);
         if (lvl == P.nt - 1) {   // the last level, recorded after the final barrier
-          for (int r = tid; r < P.nx; r += nthr)
-            S.trc[(lvl % kTraceRing) * P.nxs + r] = Y[(src_r - row0 + 2) * RS + P.pad + r + 2];
+          #pragma unroll 1
+        for (int r = tid; r < NX; r += nthr)
+            S.trc[(lvl % kTraceRing) * NXS + r] = Y[(src_r - row0 + 2) * RS + PAD + r + 2];
           flush(lvl);
         }
       }
@@ -677,14 +722,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       fence_proxy_async_all();
     }
     {
-      float* il = P.illum + static_cast<size_t>(solve) * P.nz * P.nx;
+      float* il = P.illum + static_cast<size_t>(solve) * P.nz * NX;
 #pragma unroll
       for (int k = 0; k < H; ++k)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-          const int z = myrow + k - P.pad, x = col0 + m - P.pad;
+          const int z = myrow + k - PAD, x = col0 + m - PAD;
           const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
-          if (active && z >= 0 && z < P.nz && x >= 0 && x < P.nx) il[z * P.nx + x] = a * (1.f / 144.f);
+          if (active && z >= 0 && z < P.nz && x >= 0 && x < NX) il[z * NX + x] = a * (1.f / 144.f);
         }
 #pragma unroll
       for (int k = 0; k < H; ++k)
@@ -692,15 +737,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     }
     // ---- residual (sim - obs) * mute, in place over the trace ------------
     if (rank == rec_rank) {
-      const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * P.nx;
+      const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * NX;
       const float vm = P.vmute ? P.vmute[b] : 0.f;
-      for (int i = tid; i < P.nt * P.nx; i += nthr) {
-        const int t = i / P.nx, r = i - t * P.nx;
+      for (int i = tid; i < P.nt * NX; i += nthr) {
+        const int t = i / NX, r = i - t * NX;
         const float o = ob[i];
         if (!isfinite(o)) atomicExch(P.err, static_cast<int>(SS_ERR_NONFINITE));
-        float res = trace[t * P.nxs + r] - o;
+        float res = trace[t * NXS + r] - o;
         if (P.vmute) res *= mute_weight(t, r, shot_col, P.dx, P.dt, vm, P.t_mute);
-        trace[t * P.nxs + r] = res;
+        trace[t * NXS + r] = res;
       }
       fence_proxy_async_all();   // these rows are read back by bulk copies
       __syncthreads();
@@ -712,15 +757,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
     }
     cluster_sync();
-    if (tid == 0) {   // history slab and residual row of the first adjoint step
-      const int tn = P.nt - 1, bn = tn & 1;
-      const uint32_t bar = hist_bar0 + 8u * bn;
-      const bool res_here = rank == rec_rank;
-      const uint32_t res_bytes = static_cast<uint32_t>(P.nxs * sizeof(float));
-      mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
-      bulk_load(smem_u32(bn ? S.stg[1] : S.stg[0]), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes, bar);
-      if (res_here)
-        bulk_load(smem_u32(bn ? S.res[1] : S.res[0]), trace + static_cast<size_t>(tn) * P.nxs, res_bytes, bar);
+    if (tid == 0) {   // history slabs and residual rows of the first kStages-1 adjoint steps
+      for (int tn = P.nt - 1; tn >= 0 && tn > P.nt - kStages; --tn) {
+        const int bn = tn % kStages;
+        const uint32_t bar = hist_bar0 + 8u * bn;
+        const bool res_here = rank == rec_rank;
+        const uint32_t res_bytes = static_cast<uint32_t>(NXS * sizeof(float));
+        mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
+        bulk_load(smem_u32(stage_buf(bn)), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes, bar);
+        if (res_here) bulk_load(smem_u32(res_buf(bn)), trace + static_cast<size_t>(tn) * NXS, res_bytes, bar);
+      }
     }
     {
       int i = 0;
@@ -741,8 +787,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         for (int m = 0; m < 4; ++m) {
           const int r = myrow + k, c = col0 + m;
           if (r < P.nzp - 2 && c < P.nxp - 2) {
-            const int vz = min(max(r - P.pad, 0), P.nz - 1), vx = min(max(c - P.pad, 0), P.nx - 1);
-            const float vp = v[vz * P.nx + vx];
+            const int vz = min(max(r - PAD, 0), P.nz - 1), vx = min(max(c - PAD, 0), NX - 1);
+            const float vp = v[vz * NX + vx];
             const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
             float gval = -2.f * a / vp;
             if (k == src_k && m == src_m) {
@@ -762,6 +808,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   }
   cluster_sync();     // no CTA leaves while a neighbour may still write its shared memory
 }
+
+#undef RS
+#undef NX
+#undef PAD
+#undef SW
+#undef NXS
 
 // ----------------------------------------------------------------------------
 // Small helper kernels (module-level functions of the reference)
@@ -863,6 +915,7 @@ __global__ void c2_kernel(const float* __restrict__ vel, float* __restrict__ out
 // ----------------------------------------------------------------------------
 struct Plan {
   int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads;
+  bool fast;
   size_t smem;
   int max_clusters;
   int slots;
@@ -883,23 +936,26 @@ int check_geometry(const ss_geometry* g) {
 }
 
 using SolveFn = void (*)(KParams);
-constexpr int kFastRS = 156;   // row stride of the 150-column padded OpenFWI grid (37 column groups)
 
-SolveFn kernel_for(int mode, int rs) {
-  const bool fast = rs == kFastRS;
+// The OpenFWI geometry (nx = 70, pad = 40) gets an instantiation with
+// compile-time strides; every other geometry takes them from KParams.
+bool fast_geometry(int nx, int pad) { return nx == 70 && pad == 40; }
+
+SolveFn kernel_for(int mode, bool fast) {
   switch (mode) {
-    case SS_MODE_FORWARD: return fast ? solve_kernel<SS_MODE_FORWARD, kFastRS> : solve_kernel<SS_MODE_FORWARD, 0>;
-    case SS_MODE_GRADIENT: return fast ? solve_kernel<SS_MODE_GRADIENT, kFastRS> : solve_kernel<SS_MODE_GRADIENT, 0>;
-    default: return fast ? solve_kernel<SS_MODE_IMAGES, kFastRS> : solve_kernel<SS_MODE_IMAGES, 0>;
+    case SS_MODE_FORWARD: return fast ? solve_kernel<SS_MODE_FORWARD, true> : solve_kernel<SS_MODE_FORWARD, false>;
+    case SS_MODE_GRADIENT: return fast ? solve_kernel<SS_MODE_GRADIENT, true> : solve_kernel<SS_MODE_GRADIENT, false>;
+    default: return fast ? solve_kernel<SS_MODE_IMAGES, true> : solve_kernel<SS_MODE_IMAGES, false>;
   }
 }
 
 size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj) {
   const size_t field = static_cast<size_t>(bh + 4) * rs;
   const size_t stage = adj ? static_cast<size_t>(bh) * sw : 0;
-  return (2 * field + 2 * stage + ((nt + 31) & ~31) + 32 + (2 + kTraceRing) * static_cast<size_t>(nxs)) *
+  return (2 * field + kStages * stage + ((nt + 31) & ~31) + 32 + (kStages + kTraceRing) * static_cast<size_t>(nxs) +
+          (kRowsPerThread + 4) * static_cast<size_t>(rs) + kRowsPerThread * static_cast<size_t>(sw)) *
              sizeof(float) +
-         4 * sizeof(uint64_t);
+         (kStages + 2) * sizeof(uint64_t);
 }
 
 int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
@@ -931,7 +987,8 @@ int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
   }
   if (!ok) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits shared memory for this grid");
   p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
-  const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->rs));
+  p->fast = fast_geometry(g->nx, g->pad);
+  const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->fast));
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->smem));
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   if (p->C > 8) {
@@ -1025,7 +1082,7 @@ int launch(const Plan& p, int mode, const KParams& k, cudaStream_t stream) {
   cfg.stream = stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel_for(mode, p.rs), k);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel_for(mode, p.fast), k);
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaLaunchKernelEx: ") + cudaGetErrorString(e));
   return SS_OK;
 }
