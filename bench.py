@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""RTM shot-image throughput of the B200 path, one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step"): 500 seeded OpenFWI-shaped synthetic velocity models
+(equal mix of layered / curved / faulted / textured families) x 3 laterally
+constant backgrounds (surface velocity + 0.6 / 1.0 / 1.4 x the population's
+mean depth trend) x 5 shots = 7500 shot-images, each one forward + one exact
+adjoint solve of 1000 steps on the 150x150 padded grid plus the image
+epilogue, in one kernel launch.  Observed gathers are simulated from the
+true models.  No OpenFWI data exists offline; the synthetic models have its
+shapes, spacing and velocity range.
+
+value     shot-images/s with inputs resident in HBM (CUDA events, max over ranks)
+e2e       the same metric through gpu.Sim.images with host inputs (pinned gathers),
+          host->device and device->host copies inside the timed region
+roofline  FP32 CUDA-core throughput: 0.81 GFLOP per shot-image (150^2 cells x
+          1000 steps x 36 flops) over the launch time, against an FMA peak
+          measured live on this GPU
+cpu_baseline  the oracle's float32 restatement of the reference CPU path
+          (PyTorch eager, all host threads) on a bounded sample
+
+With torchrun, every rank simulates its own 500 models (weak scaling); the
+ranks exchange nothing on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'RTM shot-images/s (70x70, 1000 steps)'
+UNIT = 'shot-images/s'
+N_MODELS = 500
+RHOS = (0.6, 1.0, 1.4)
+FLOP_PER_SHOT_IMAGE = 150 * 150 * 1000 * 36
+WORKLOAD = ('RTM images: 500 seeded OpenFWI-shaped synthetic models x 3 backgrounds x 5 shots = 7500 shot-images, '
+            '70x70 cells + 40-cell absorbing pad, 1000 steps, one launch')
+CPU_SAMPLE_ROWS = 6          # background rows (x 5 shots) per CPU measurement
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__.split('\n')[0])
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
+    ap.add_argument('--models', type=int, default=N_MODELS, help='velocity models per GPU')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+def population_slice(start, stop, total):
+    """Models [start, stop) of a seeded population of `total` (family mix as synth.population)."""
+    from shotsweep_b200 import synth
+    return np.stack([synth.model(synth.FAMILIES[i * len(synth.FAMILIES) // total], [1, i]) for i in range(start, stop)])
+
+
+def backgrounds_for(models, trend):
+    """Per model: surface velocity (top-row mean) + rho x trend, clipped, laterally constant (3 rows each)."""
+    v_s = models[:, 0, :].astype(np.float64).mean(1)
+    rows = [np.tile(np.clip(v + r * trend, 1500.0, 4500.0)[:, None], (1, models.shape[2])) for v in v_s for r in RHOS]
+    return np.stack(rows), np.repeat(v_s, len(RHOS))
+
+
+def depth_trend(models):
+    m = np.asarray(models, np.float64)
+    return (m.mean(2) - m[:, :1, :].mean(2)).mean(0)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples every 200 ms while the timed region runs."""
+    QUERY = ('index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, bus_id):
+        self.bus_id = (bus_id or '').lower()
+        self.file = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--query-gpu={self.QUERY}', '--format=csv,noheader,nounits',
+                                          '-lms', '200'], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
+        for line in self.file:
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 10:
+                continue
+            if self.bus_id and self.bus_id not in f[1].lower():
+                continue
+            try:
+                sm.append(float(f[2]))
+                mx = float(f[3])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[6:10]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['no samples']}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def fp32_peak(device):
+    """Measured FP32 FMA throughput (TFLOP/s): max of scalar and packed FP32x2 probes over all SMs."""
+    import ctypes
+    import torch
+    from shotsweep_b200 import _lib
+    L = _lib.load()
+    out = torch.zeros(1, device=device)
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    best = 0.0
+    for packed in (0, 1):
+        for _ in range(2):
+            flops = ctypes.c_double()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.check(L.ss_fp32_probe(_lib.ptr(out), sms * 8, 20000, packed, ctypes.byref(flops),
+                                       _lib.stream_handle(device)), 'ss_fp32_probe')
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def dram_bytes_per_solve():
+    """Per-solve DRAM traffic of the images kernel from the committed ncu summary, or None."""
+    path = ROOT / 'profiles' / 'images_kernel_70x70.md'
+    if not path.exists():
+        return None
+    m = re.search(r'dram_bytes_per_solve\s*=\s*([0-9.eE+]+)', path.read_text())
+    return float(m.group(1)) if m else None
+
+
+def cpu_port_rate(obs_rows, bgs, vm, rows, threads, repeats=3):
+    """shot-images/s of the oracle's float32 CPU restatement of Sim.images on `rows` background rows."""
+    import torch
+    from oracle import oracle as O
+    torch.set_num_threads(threads)
+    sim = O.OracleSim(dtype=torch.float32)
+    sim.images(bgs[:1], obs_rows[:1], v_mute=vm[:1])            # warm-up (allocator, threads)
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        sim.images(bgs[:rows], obs_rows[:rows], v_mute=vm[:rows])
+        times.append(time.perf_counter() - t0)
+    return rows * 5 / statistics.median(times)
+
+
+def run_reference(args):
+    """CPU arm: the oracle port of the reference path on the host cores, rank 0 only."""
+    rank = int(os.environ.get('RANK', 0))
+    if rank != 0:
+        return 0
+    import torch
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    models = population_slice(0, 2, N_MODELS)
+    trend = depth_trend(population_slice(0, N_MODELS, N_MODELS))
+    bgs, vm = backgrounds_for(models, trend)
+    osim = O.OracleSim(dtype=torch.float32)
+    obs = np.repeat(osim.gathers(models.astype(np.float64)), len(RHOS), 0)
+    rows = CPU_SAMPLE_ROWS
+    for _ in range(args.warmup):
+        osim.images(bgs[:rows], obs[:rows], v_mute=vm[:rows])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        osim.images(bgs[:rows], obs[:rows], v_mute=vm[:rows])
+    elapsed = time.perf_counter() - t0
+    value = rows * 5 * args.steps / elapsed
+    sample = (f'{rows} background rows x 5 shots = {rows * 5} shot-images per step from the same workload, '
+              f'float32 PyTorch eager on {threads} host threads')
+    print(json.dumps({
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': elapsed / args.steps * 1e3,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': {'workload': WORKLOAD, 'sample': sample},
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': threads, 'kind': 'port', 'sample': sample},
+        'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    from shotsweep_b200 import dist as D
+    from shotsweep_b200 import engine, gpu
+    rank, world, local = D.init('nccl' if args.gpus > 1 else 'gloo', timeout_s=300)
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    per = args.models
+    a, b = D.shard(per * world, rank, world)
+    models = population_slice(a, b, per * world) if world > 1 else population_slice(0, per, per)
+    trend = depth_trend(population_slice(0, N_MODELS, N_MODELS))
+    bgs, vm = backgrounds_for(models, trend)
+    n_rows = len(bgs)
+    shot_images = n_rows * 5
+
+    sim = gpu.Sim(device=dev)
+    eng = sim.engine
+    w = engine.scaled_wavelet(gpu.RICKER, dev)
+    obs_models = eng.forward(torch.tensor(models, dtype=torch.float32, device=dev), w)
+    obs = obs_models.repeat_interleave(len(RHOS), dim=0).contiguous()
+    del obs_models
+    bg_d = torch.tensor(bgs, dtype=torch.float32, device=dev)
+    vm_d = torch.tensor(vm, dtype=torch.float32, device=dev)
+    img = torch.empty(n_rows, 5, 70, 70, dtype=torch.float32, device=dev)
+    illum = torch.empty_like(img)
+
+    def step():
+        eng.images(bg_d, w, obs, vm_d, out=(img, illum))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    eng.status()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    props = torch.cuda.get_device_properties(dev)
+    bus = None
+    if hasattr(props, 'pci_bus_id'):
+        bus = f'{getattr(props, "pci_domain_id", 0):08X}:{props.pci_bus_id:02X}:{getattr(props, "pci_device_id", 0):02X}.0'
+    D.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(bus) as clk:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record()
+        for e0, e1 in events:
+            e0.record()
+            step()
+            e1.record()
+        t_all1.record()
+        torch.cuda.synchronize()
+    D.barrier()
+    eng.status()
+    elapsed_ms = D.reduce(t_all0.elapsed_time(t_all1), 'max', dev if world > 1 else None)
+    launch_ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in events)
+    value = world * shot_images * args.steps / (elapsed_ms * 1e-3)
+    clocks = clk.summary()
+
+    # end to end through the public API: pinned host gathers in, numpy images out
+    obs_host = obs.cpu().pin_memory()
+    h2d = obs_host.numel() * 4 + bgs.size * 8 + vm.size * 8
+    d2h = img.numel() * 4 * 2
+    sim.images(bgs, obs_host, v_mute=vm)
+    D.barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        sim.images(bgs, obs_host, v_mute=vm)
+    e2e_s = D.reduce(time.perf_counter() - t0, 'max', dev if world > 1 else None)
+    e2e = world * shot_images * e2e_steps / e2e_s
+
+    peak = fp32_peak(dev)
+    achieved = FLOP_PER_SHOT_IMAGE * shot_images / (launch_ms * 1e-3) / 1e12
+    per_solve = dram_bytes_per_solve()
+    roofline = {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
+                'traffic': per_solve * shot_images if per_solve else None,
+                'peak_source': 'measured live: max of scalar FFMA and packed FFMA2 probes on all SMs '
+                               '(MEASURED_PEAKS.json has no FP32 figure)',
+                'algorithmic': '36 flops per padded cell per step (16 forward + 20 adjoint), 150^2 cells, 1000 steps; '
+                               'traffic = ncu dram bytes per solve (profiles/images_kernel_70x70.md) x solves'}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        obs_rows = obs[:CPU_SAMPLE_ROWS].cpu().double().numpy()
+        rate = cpu_port_rate(obs_rows, bgs, vm, CPU_SAMPLE_ROWS, threads)
+        cpu = {'value': rate, 'unit': UNIT, 'cores': threads, 'kind': 'port',
+               'sample': f'{CPU_SAMPLE_ROWS} background rows x 5 shots of the same workload (median of 3), '
+                         f'oracle float32 PyTorch-eager restatement of Sim.images on {threads} threads'}
+    if rank == 0:
+        print(json.dumps({
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': elapsed_ms / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+            'data': 'synthetic: seeded OpenFWI-shaped velocity models, gathers simulated from the true models',
+            'config': {'workload': WORKLOAD, 'models_per_gpu': per, 'backgrounds_per_model': len(RHOS),
+                       'shots': 5, 'shot_images_per_gpu': shot_images, 'nz': 70, 'nx': 70, 'nt': 1000, 'pad': 40,
+                       'parallelism': f'{world} independent ranks (weak scaling, no data-path collective)',
+                       'l2': 'inputs larger than L2 (2.1 GB of gathers per step per GPU)',
+                       'plan': eng.plan(n_rows, 2)},
+            'roofline': roofline, 'cpu_baseline': cpu,
+            'e2e': {'value': e2e, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
+                    'api': 'shotsweep_b200.gpu.Sim.images (pinned torch gathers, numpy velocities in; numpy out)'},
+            'clocks': clocks, 'gpu_launches': args.steps,
+        }), flush=True)
+    D.finish()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.warmup < 0 or args.steps < 1:
+        raise SystemExit('--steps must be positive and --warmup non-negative')
+    if args.impl == 'reference':
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -145,6 +145,14 @@ int32_t ss_mute_weights(const ss_geometry* geom, int32_t n_models, const float* 
  * [n_models, nz+2pad, nx+2pad] (gpu.py:105-107). */
 int32_t ss_c2_field(const ss_geometry* geom, int32_t n_models, const float* vel, float* out, void* stream);
 
+/* FP32 throughput probe (no counterpart in the reference: a diagnostic that
+ * supplies the roofline denominator of the FP32 stencil kernels).  Launches
+ * `blocks` x 256 threads, each running 8 independent FMA chains of `iters`
+ * steps, scalar (packed = 0) or packed FP32x2 (packed = 1); *flops receives
+ * the floating-point operations the launch performs (an FMA counts 2).  The
+ * caller times the launch on `stream`; `out` must hold one float. */
+int32_t ss_fp32_probe(float* out, int32_t blocks, int32_t iters, int32_t packed, double* flops, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,8 @@ _SIGNATURES = {
                                                   ctypes.c_int32, _P]),
     'ss_mute_weights': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, ctypes.c_float, _P, _P]),
     'ss_c2_field': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P]),
+    'ss_fp32_probe': (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.POINTER(ctypes.c_double), _P]),
 }
 
 _lock = threading.Lock()

@@ -910,6 +910,31 @@ __global__ void c2_kernel(const float* __restrict__ vel, float* __restrict__ out
   }
 }
 
+// FP32 throughput probe: 8 independent FMA chains per thread, scalar or
+// packed FP32x2, for the roofline denominator of the stencil kernels.
+template <bool PACKED>
+__global__ void __launch_bounds__(256) fp32_probe_kernel(float* out, int iters) {
+  float2 a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = make_float2(threadIdx.x * 1e-3f + j, j * 0.5f);
+  const float2 m = make_float2(0.999999f, 0.999998f), c = make_float2(1e-6f, 2e-6f);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (PACKED) {
+        a[j] = __ffma2_rn(a[j], m, c);
+      } else {
+        a[j].x = fmaf(a[j].x, m.x, c.x);
+        a[j].y = fmaf(a[j].y, m.y, c.y);
+      }
+    }
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc += a[j].x + a[j].y;
+  if (acc == 12345.678f) out[0] = acc;   // keeps the chains live; practically never stores
+}
+
 // ----------------------------------------------------------------------------
 // Host side: plans, workspace, launches
 // ----------------------------------------------------------------------------
@@ -1265,6 +1290,19 @@ int32_t ss_mute_weights(const ss_geometry* geom, int32_t n_models, const float* 
   mute_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, v_mute, n_models, geom->n_shots,
                                                                               geom->nt, geom->nx, k);
   SS_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_fp32_probe(float* out, int32_t blocks, int32_t iters, int32_t packed, double* flops, void* stream) {
+  g_last_error.clear();
+  if (!out || blocks < 1 || iters < 1 || !flops) return fail(SS_ERR_INVALID, "bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (packed)
+    fp32_probe_kernel<true><<<blocks, 256, 0, st>>>(out, iters);
+  else
+    fp32_probe_kernel<false><<<blocks, 256, 0, st>>>(out, iters);
+  SS_CUDA(cudaGetLastError());
+  *flops = 2.0 * 16.0 * static_cast<double>(iters) * 256.0 * blocks;   // 16 FMAs per thread per iteration
   return SS_OK;
 }
 
