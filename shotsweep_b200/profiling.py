@@ -1,0 +1,46 @@
+"""Small fixed workload for profiling the solve kernels with ncu.
+
+    python -m shotsweep_b200.profiling [n_models]
+
+Runs, on cuda:0, with `n_models` seeded synthetic models (default 9, i.e.
+45 solves, one round of three-CTA clusters on a B200):
+  1. forward of the true models (observed gathers),
+  2. images, 3. forward          (warm-up),
+  4. forward, 5. images          (the launches to capture: ncu -s 3 -c 2),
+and prints their CUDA-event times.
+"""
+import sys
+
+import numpy as np
+import torch
+
+from . import engine, gpu, synth
+
+
+def main(n_models=9):
+    eng = engine.Engine(engine.geometry())
+    dev = eng.device
+    w = engine.scaled_wavelet(gpu.RICKER, dev)
+    vt = torch.tensor(synth.population(max(n_models, 4))[:n_models], dtype=torch.float32, device=dev)
+    obs = eng.forward(vt, w)
+    bg = torch.tensor(np.stack([np.tile(np.linspace(1600, 3600, 70)[:, None], (1, 70))] * n_models),
+                      dtype=torch.float32, device=dev)
+    vm = torch.full((n_models,), 1700.0, device=dev)
+    eng.images(bg, w, obs, vm)
+    eng.forward(vt, w)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    eng.forward(vt, w)
+    ev[1].record()
+    ev[2].record()
+    eng.images(bg, w, obs, vm)
+    ev[3].record()
+    torch.cuda.synchronize()
+    eng.status()
+    print(f'models={n_models} solves={5 * n_models} forward {ev[0].elapsed_time(ev[1]):.3f} ms '
+          f'images {ev[2].elapsed_time(ev[3]):.3f} ms')
+
+
+if __name__ == '__main__':
+    main(int(sys.argv[1]) if len(sys.argv) > 1 else 9)
