@@ -145,6 +145,32 @@ int32_t ss_mute_weights(const ss_geometry* geom, int32_t n_models, const float* 
  * [n_models, nz+2pad, nx+2pad] (gpu.py:105-107). */
 int32_t ss_c2_field(const ss_geometry* geom, int32_t n_models, const float* vel, float* out, void* stream);
 
+/* RTM images without any device allocation: no counterpart in the
+ * reference.  Some callers cannot call cudaMalloc when they need images: a
+ * plugin host that hands over only input and output buffers, a framework
+ * whose caching allocator owns all device memory, or a service that must not
+ * allocate after start-up.  This entry point computes exactly what ss_images
+ * computes (same arguments without the workspace), taking its scratch from a
+ * fixed 32 MiB (33554432-byte) device array inside the library, which every
+ * GPU that loads the library holds until the process exits.
+ *   - Geometries whose single-solve scratch (per-step history, receiver
+ *     traces, padded gradient) exceeds 32 MiB are rejected with
+ *     SS_ERR_UNSUPPORTED; the 70x70 / 1000-step OpenFWI geometry needs about
+ *     90 MB per solve and so needs ss_images.  Smaller problems run with as
+ *     many solves in flight as fit in the array.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call shares the one array, and it keeps the previous call's
+ *     contents: calls that overlap on the GPU (other streams, other host
+ *     threads) race and corrupt each other's results.
+ *   - The call waits for its work on `stream` and returns the device-side
+ *     status (SS_ERR_NONFINITE, SS_ERR_TIMEOUT), since there is no workspace
+ *     to read it from afterwards. */
+int32_t ss_images_noalloc(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                          const float* obs, const float* v_mute, float t_mute, float eps, int32_t laplacian,
+                          float* img, float* illum, float* grad, void* stream);
+
 /* FP32 throughput probe (no counterpart in the reference: a diagnostic that
  * supplies the roofline denominator of the FP32 stencil kernels).  Launches
  * `blocks` x 256 threads, each running 8 independent FMA chains of `iters`

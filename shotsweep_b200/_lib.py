@@ -66,6 +66,8 @@ _SIGNATURES = {
     'ss_c2_field': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P]),
     'ss_fp32_probe': (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_double), _P]),
+    'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
+                                           ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }
 
 _lock = threading.Lock()

@@ -1155,6 +1155,40 @@ int grid_for(long long total) {
   return static_cast<int>(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
 }
 
+// ----------------------------------------------------------------------------
+// Allocation-free images: scratch in a file-scope device array
+// ----------------------------------------------------------------------------
+// Some callers cannot allocate device memory when they call us: a plugin
+// host that hands out only input/output buffers, a framework whose caching
+// allocator owns all device memory, or a process that must not allocate
+// after start-up.  ss_images_noalloc serves them with the images kernel and
+// a fixed 32 MiB scratch array that every GPU loading this library holds
+// until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[64] = {};   // device address of g_noalloc_scratch, per device index
+
+// Device address of the scratch array on the current device.  The first call
+// on a device looks it up with cudaGetSymbolAddress (the host-side name of the
+// array is only a stand-in, not a device address) and caches it.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  SS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SS_ERR_UNSUPPORTED, "device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_address[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(SS_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_noalloc_address[dev] = p;
+  }
+  *out = g_noalloc_address[dev];
+  return SS_OK;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1290,6 +1324,64 @@ int32_t ss_mute_weights(const ss_geometry* geom, int32_t n_models, const float* 
   mute_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(out, v_mute, n_models, geom->n_shots,
                                                                               geom->nt, geom->nx, k);
   SS_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_images_noalloc(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                          const float* obs, const float* v_mute, float t_mute, float eps, int32_t laplacian,
+                          float* img, float* illum, float* grad, void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (n_models < 1) return fail(SS_ERR_INVALID, "n_models must be positive");
+  if (!vel || !wavelet || !obs || !illum || !img) return fail(SS_ERR_INVALID, "vel, wavelet, obs, img and illum are required");
+  if (!(eps > 0.f)) return fail(SS_ERR_INVALID, "illumination regularization eps must be positive");
+  void* scratch = nullptr;
+  rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  Plan p;
+  rc = make_plan(geom, SS_MODE_IMAGES, n_models * geom->n_shots, &p);
+  if (rc) return rc;
+  // Fewer solves in flight until their scratch fits the fixed array.
+  WsLayout L = ws_layout(geom, p, SS_MODE_IMAGES);
+  while (L.total > kNoAllocScratchBytes && p.slots > 1) {
+    --p.slots;
+    L = ws_layout(geom, p, SS_MODE_IMAGES);
+  }
+  if (L.total > kNoAllocScratchBytes)
+    return fail(SS_ERR_UNSUPPORTED, "one solve of this geometry needs " + std::to_string(L.total) +
+                                        " bytes of scratch, more than the 33554432-byte allocation-free array; "
+                                        "use ss_images with a workspace");
+  unsigned char* w = static_cast<unsigned char*>(scratch);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The array keeps the previous call's contents; only the status word must
+  // start at zero (every other scratch byte is written before it is read).
+  SS_CUDA(cudaMemsetAsync(w + L.err, 0, 256, st));
+  KParams k = base_params(geom, p, n_models);
+  k.vel = vel;
+  k.wav = wavelet;
+  k.obs = obs;
+  k.vmute = v_mute;
+  k.t_mute = t_mute;
+  k.trace = reinterpret_cast<float*>(w + L.trace);
+  k.illum = illum;
+  k.grad_per_slot = grad == nullptr;
+  k.grad = grad ? grad : reinterpret_cast<float*>(w + L.grad);
+  k.img = img;
+  k.gpad = reinterpret_cast<float*>(w + L.gpad);
+  k.hist = reinterpret_cast<float*>(w + L.hist);
+  k.eps = eps;
+  k.laplacian = laplacian;
+  k.err = reinterpret_cast<int*>(w + L.err);
+  k.ckpt_interval = 1;
+  rc = launch(p, SS_MODE_IMAGES, k, st);
+  if (rc) return rc;
+  // No workspace to read a status from later: wait here and report it.
+  int flag = 0;
+  SS_CUDA(cudaMemcpyAsync(&flag, w + L.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SS_CUDA(cudaStreamSynchronize(st));
+  if (flag == SS_ERR_NONFINITE) return fail(flag, "observations must be finite");
+  if (flag != 0) return fail(flag, "a device-side bounded wait ran out (history copy did not complete)");
   return SS_OK;
 }
 
