@@ -68,7 +68,8 @@ typedef struct ss_geometry {
 typedef enum ss_mode {
     SS_MODE_FORWARD = 0,   /* gathers only                         */
     SS_MODE_GRADIENT = 1,  /* forward + adjoint -> gradient, illum  */
-    SS_MODE_IMAGES = 2     /* gradient + image epilogue             */
+    SS_MODE_IMAGES = 2,    /* gradient + image epilogue             */
+    SS_MODE_SEGMENT = 3    /* one checkpointed adjoint segment      */
 } ss_mode;
 
 /* Library version string. */
@@ -126,6 +127,29 @@ int32_t ss_images(const ss_geometry* geom, int32_t n_models, const float* vel, c
                   const float* obs, const float* v_mute, float t_mute, float eps, int32_t laplacian,
                   float* img, float* illum, float* grad,
                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Checkpointed adjoint for differentiation (torch.autograd): the forward
+ * keeps only the states (p[t-1], p[t]) every K = ckpt_interval steps
+ * (ss_forward with ckpt), and the gradient is rebuilt segment by segment,
+ * last segment first.  Replaces the checkpoint/recompute loop of
+ * Sim._gradient (gpu.py:169-184) with a given adjoint source instead of the
+ * muted residual.  Per segment k (levels [kK, min((k+1)K, nt))):
+ *   res        [n_models, n_shots, nt, nx]     adjoint source dJ/d(gathers)
+ *   theta      [n_models, n_shots, 2, nz+2pad, nx+2pad]  scaled adjoint state,
+ *              zero before the last segment, carried in place between calls
+ *   gacc       [n_models, n_shots, nz+2pad, nx+2pad]     accumulator, zero at start
+ *   illum_acc  [n_models, n_shots, nz, nx]               accumulator, zero at start
+ *   src_acc    [n_models, n_shots]                       accumulator, zero at start
+ * Workspace: ss_segment_workspace_bytes.  After segment 0, ss_gradient_finish
+ * turns the accumulators into the per-shot gradient and illumination
+ * (the fold and source term of gpu.py:185-187). */
+size_t ss_segment_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t ckpt_interval);
+int32_t ss_adjoint_segment(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                           const float* ckpt, int32_t ckpt_interval, int32_t seg_index, const float* res,
+                           float* theta, float* gacc, float* illum_acc, float* src_acc,
+                           void* workspace, size_t workspace_bytes, void* stream);
+int32_t ss_gradient_finish(const ss_geometry* geom, int32_t n_models, const float* vel, const float* gacc,
+                           const float* src_acc, const float* illum_acc, float* grad, float* illum, void* stream);
 
 /* Module helpers (gpu.py:33-67, 142-150, 105-107) on device arrays whose last
  * two axes are (n0, n1); `batch` is the product of the leading axes. */

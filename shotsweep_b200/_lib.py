@@ -15,7 +15,7 @@ LIB_PATH = Path(__file__).resolve().parent / 'libshotsweep.so'
 MAX_SHOTS = 16
 
 OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_TIMEOUT, ERR_WORKSPACE, ERR_NONFINITE = 0, -1, -2, -3, -4, -5, -6
-MODE_FORWARD, MODE_GRADIENT, MODE_IMAGES = 0, 1, 2
+MODE_FORWARD, MODE_GRADIENT, MODE_IMAGES, MODE_SEGMENT = 0, 1, 2, 3
 
 
 class Geometry(ctypes.Structure):
@@ -66,6 +66,10 @@ _SIGNATURES = {
     'ss_c2_field': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P]),
     'ss_fp32_probe': (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_double), _P]),
+    'ss_segment_workspace_bytes': (ctypes.c_size_t, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32]),
+    'ss_adjoint_segment': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, ctypes.c_int32,
+                                            ctypes.c_int32, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
+    'ss_gradient_finish': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

@@ -193,6 +193,13 @@ struct KParams {
   float eps;
   int laplacian;
   int* err;
+  // segment mode (checkpointed adjoint): levels [seg_start, seg_start + seg_steps)
+  int seg_start, seg_steps, seg_index, hist_steps;
+  float* theta;        // [solve][2][nzp][nxp]: in (th[e+1], th[e+2]), out (th[s], th[s+1])
+  float* gacc;         // [solve][nzp][nxp]: += -sum_t th*S over the segment
+  float* illum_acc;    // [solve][nz][nx]: += sum_t S^2 over the segment
+  float* src_acc_io;   // [solve]: += sum_t th(source cell) * w[t]
+  const float* res_in; // [solve][nt][nx]: adjoint source (the gathers' cotangent)
 };
 
 struct Smem {
@@ -519,7 +526,11 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
 
   const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * SW * sizeof(float));
-  const size_t hist_slot = static_cast<size_t>(P.nt) * P.C * P.bh * SW;
+  const size_t hist_slot = static_cast<size_t>(P.hist_steps) * P.C * P.bh * SW;
+  constexpr bool SEG = MODE == SS_MODE_SEGMENT;
+  const int lvl_lo = SEG ? P.seg_start : 0;                  // first level of the time range
+  const int n_steps = SEG ? P.seg_steps : P.nt;               // steps of each sweep
+  const int lvl_hi = lvl_lo + n_steps - 1;
   float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * SW
                                : nullptr;
   const size_t hist_step = static_cast<size_t>(P.C) * P.bh * SW;
@@ -597,17 +608,18 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
                          const bool fwd) {
       const float* X = cur ? S.f[1] : S.f[0];
       float* Y = cur ? S.f[0] : S.f[1];
-      const bool more = step + 1 < P.nt;
+      const bool more = step + 1 < n_steps;
       const int bi = lvl % kStages;
       if (tid == 0 && more) {
         if (halo_bytes) mbar_expect_tx(halo_bar0 + 8u * (cur ^ 1), halo_bytes);
-        if (!fwd && lvl - (kStages - 1) >= 0) {   // history slab (and residual row) kStages-1 steps ahead
+        if (!fwd && lvl - (kStages - 1) >= lvl_lo) {   // history slab (and residual row) kStages-1 steps ahead
           const int tn = lvl - (kStages - 1), bn = tn % kStages;
           const uint32_t bar = hist_bar0 + 8u * bn;
           const bool res_here = rank == rec_rank;
           const uint32_t res_bytes = static_cast<uint32_t>(NXS * sizeof(float));
           mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
-          bulk_load(smem_u32(stage_buf(bn)), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes, bar);
+          bulk_load(smem_u32(stage_buf(bn)), hist_mine + static_cast<size_t>(tn - lvl_lo) * hist_step, stage_bytes,
+                    bar);
           if (res_here) bulk_load(smem_u32(res_buf(bn)), trace + static_cast<size_t>(tn) * NXS, res_bytes, bar);
         }
       }
@@ -636,7 +648,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         hist_phase ^= 1u << bi;
       }
       const bool push_up = more && edge_up, push_dn = more && edge_dn;
-      if (fwd && rank == rec_rank && step > 0) {
+      if (!SEG && fwd && rank == rec_rank && step > 0) {
         // receivers at every model column (gpu.py:134): the level recorded at
         // the previous step is now the read-only field X
         #pragma unroll 1
@@ -678,8 +690,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       }
       __syncthreads();
       if (fwd && ADJ && tid == 0)
-        bulk_store(hist_mine + static_cast<size_t>(lvl) * hist_step, smem_u32(stage_buf(bi)), stage_bytes);
-      if (fwd && rank == rec_rank) {
+        bulk_store(hist_mine + static_cast<size_t>(lvl - lvl_lo) * hist_step, smem_u32(stage_buf(bi)), stage_bytes);
+      if (!SEG && fwd && rank == rec_rank) {
         // The ring holds the receiver rows [flushed, lvl-1] (level lvl-1 was
         // recorded at this step's start).  A full ring, and at the end every
         // remaining row, goes to global memory, coalesced.
@@ -704,14 +716,46 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       }
     };
 
-    // ================= forward: t = 0 .. nt-1 =============================
-    {
-      int t = 0;
-      for (; t + 1 < P.nt; t += 2) {
-        tile_step(A, B, t, t, 0, true);
-        tile_step(B, A, t + 1, t + 1, 1, true);
+    // Segment mode: the sweep starts from stored fields (a forward checkpoint,
+    // or the carried adjoint state) instead of zero; shared field f[0] gets the
+    // current level for the whole band and its halo rows straight from them.
+    auto load_state = [&](const float* cur_lvl, const float* prev_lvl) {
+#pragma unroll 1
+      for (int i = tid; i < (P.bh + 4) * RS; i += nthr) {
+        const int r = row0 - 2 + i / RS, c = i % RS - 2;
+        S.f[0][i] = (r >= 0 && r < P.nzp - 2 && c >= 0 && c < P.nxp - 2) ? cur_lvl[static_cast<size_t>(r) * P.nxp + c] : 0.f;
       }
-      if (t < P.nt) tile_step(A, B, t, t, 0, true);
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        float a[4], p[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int r = myrow + k, c = col0 + m;
+          const bool in = active && r < P.nzp - 2 && c < P.nxp - 2;
+          a[m] = in ? cur_lvl[static_cast<size_t>(r) * P.nxp + c] : 0.f;
+          p[m] = in ? prev_lvl[static_cast<size_t>(r) * P.nxp + c] : 0.f;
+        }
+        A[k][0] = make_float2(a[0], a[1]);
+        A[k][1] = make_float2(a[2], a[3]);
+        B[k][0] = make_float2(p[0], p[1]);
+        B[k][1] = make_float2(p[2], p[3]);
+      }
+    };
+    if (SEG) {
+      const size_t fld = static_cast<size_t>(P.nzp) * P.nxp;
+      const float* ck = P.ckpt + (static_cast<size_t>(solve) * P.n_ckpt + P.seg_index) * 2 * fld;
+      load_state(ck + fld, ck);   // (p[s], p[s-1])
+      cluster_sync();
+    }
+
+    // ================= forward: t = lvl_lo .. lvl_hi ======================
+    {
+      int i = 0;
+      for (; i + 1 < n_steps; i += 2) {
+        tile_step(A, B, i, lvl_lo + i, 0, true);
+        tile_step(B, A, i + 1, lvl_lo + i + 1, 1, true);
+      }
+      if (i < n_steps) tile_step(A, B, i, lvl_lo + i, 0, true);
     }
 
     if (MODE == SS_MODE_FORWARD) continue;
@@ -729,14 +773,28 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         for (int m = 0; m < 4; ++m) {
           const int z = myrow + k - PAD, x = col0 + m - PAD;
           const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
-          if (active && z >= 0 && z < P.nz && x >= 0 && x < NX) il[z * NX + x] = a * (1.f / 144.f);
+          if (active && z >= 0 && z < P.nz && x >= 0 && x < NX) {
+            if (SEG)
+              P.illum_acc[static_cast<size_t>(solve) * P.nz * NX + z * NX + x] += a;
+            else
+              il[z * NX + x] = a * (1.f / 144.f);
+          }
         }
 #pragma unroll
       for (int k = 0; k < H; ++k)
         acc[k][0] = acc[k][1] = A[k][0] = A[k][1] = B[k][0] = B[k][1] = make_float2(0.f, 0.f);
     }
     // ---- residual (sim - obs) * mute, in place over the trace ------------
-    if (rank == rec_rank) {
+    if (SEG && rank == rec_rank) {   // segment mode: the adjoint source is given
+      const float* rg = P.res_in + static_cast<size_t>(solve) * P.nt * NX;
+#pragma unroll 1
+      for (int i = tid; i < n_steps * NX; i += nthr) {
+        const int t = lvl_lo + i / NX, r = i % NX;
+        trace[t * NXS + r] = rg[static_cast<size_t>(t) * NX + r];
+      }
+      fence_proxy_async_all();
+      __syncthreads();
+    } else if (rank == rec_rank) {
       const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * NX;
       const float vm = P.vmute ? P.vmute[b] : 0.f;
       for (int i = tid; i < P.nt * NX; i += nthr) {
@@ -751,30 +809,59 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       __syncthreads();
     }
 
-    // ================= adjoint: t = nt-1 .. 0 =============================
+    // ================= adjoint: t = lvl_hi .. lvl_lo ======================
     for (size_t i = tid; i < field_floats / 2; i += nthr) {
       reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
       reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
     }
+    float* th_io = SEG ? P.theta + static_cast<size_t>(solve) * 2 * P.nzp * P.nxp : nullptr;
+    if (SEG) {
+      __syncthreads();   // the zeroing above and load_state map threads to f[0] differently
+      load_state(th_io, th_io + static_cast<size_t>(P.nzp) * P.nxp);   // (th[e+1], th[e+2])
+    }
     cluster_sync();
     if (tid == 0) {   // history slabs and residual rows of the first kStages-1 adjoint steps
-      for (int tn = P.nt - 1; tn >= 0 && tn > P.nt - kStages; --tn) {
+      for (int tn = lvl_hi; tn >= lvl_lo && tn > lvl_hi - (kStages - 1); --tn) {
         const int bn = tn % kStages;
         const uint32_t bar = hist_bar0 + 8u * bn;
         const bool res_here = rank == rec_rank;
         const uint32_t res_bytes = static_cast<uint32_t>(NXS * sizeof(float));
         mbar_expect_tx(bar, stage_bytes + (res_here ? res_bytes : 0u));
-        bulk_load(smem_u32(stage_buf(bn)), hist_mine + static_cast<size_t>(tn) * hist_step, stage_bytes, bar);
+        bulk_load(smem_u32(stage_buf(bn)), hist_mine + static_cast<size_t>(tn - lvl_lo) * hist_step, stage_bytes,
+                  bar);
         if (res_here) bulk_load(smem_u32(res_buf(bn)), trace + static_cast<size_t>(tn) * NXS, res_bytes, bar);
       }
     }
     {
       int i = 0;
-      for (; i + 1 < P.nt; i += 2) {
-        tile_step(A, B, i, P.nt - 1 - i, 0, false);
-        tile_step(B, A, i + 1, P.nt - 2 - i, 1, false);
+      for (; i + 1 < n_steps; i += 2) {
+        tile_step(A, B, i, lvl_hi - i, 0, false);
+        tile_step(B, A, i + 1, lvl_hi - 1 - i, 1, false);
       }
-      if (i < P.nt) tile_step(A, B, i, P.nt - 1 - i, 0, false);
+      if (i < n_steps) tile_step(A, B, i, lvl_hi - i, 0, false);
+    }
+    if (SEG) {
+      // carry the adjoint state (th[s], th[s+1]) and the accumulators to the next segment
+      const size_t fld = static_cast<size_t>(P.nzp) * P.nxp;
+      float* g = P.gacc + static_cast<size_t>(solve) * fld;
+#pragma unroll
+      for (int k = 0; k < H; ++k)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int r = myrow + k, c = col0 + m;
+          if (active && r < P.nzp - 2 && c < P.nxp - 2) {
+            const size_t o = static_cast<size_t>(r) * P.nxp + c;
+            const float a = (m & 1) ? A[k][m >> 1].y : A[k][m >> 1].x;
+            const float bv = (m & 1) ? B[k][m >> 1].y : B[k][m >> 1].x;
+            th_io[o] = (n_steps & 1) ? bv : a;          // newest level, th[s]
+            th_io[fld + o] = (n_steps & 1) ? a : bv;    // th[s+1]
+            g[o] += (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
+          }
+        }
+      if (src_k >= 0) P.src_acc_io[solve] += src_acc;
+      __threadfence();
+      cluster_sync();
+      continue;
     }
 
     // ---- padded gradient 2/v * sum_t th*S(p), plus the source term -------
@@ -910,6 +997,51 @@ __global__ void c2_kernel(const float* __restrict__ vel, float* __restrict__ out
   }
 }
 
+// Gradient from the segment accumulators: g_pad = -2 gacc / v on interior
+// cells plus the source-strength term, folded onto the model edges
+// (gpu.py:56-67, 185-187); illumination = sum S^2 / 144.
+__global__ void finish_kernel(KParams P, const float* __restrict__ gacc, const float* __restrict__ src_acc,
+                              const float* __restrict__ illum_acc, float* __restrict__ grad, float* __restrict__ illum) {
+  const long long total = static_cast<long long>(P.n_solves) * P.nz * P.nx;
+  const int nzp = P.nzp, nxp = P.nxp, pad = P.pad;
+  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
+       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(idx % P.nx);
+    const int z = static_cast<int>((idx / P.nx) % P.nz);
+    const int solve = static_cast<int>(idx / (static_cast<long long>(P.nz) * P.nx));
+    const int b = solve / P.n_shots, s = solve - b * P.n_shots;
+    const float* v = P.vel + static_cast<size_t>(b) * P.nz * P.nx;
+    const float* G = gacc + static_cast<size_t>(solve) * nzp * nxp;
+    auto at = [&](int i, int j) -> float {
+      if (i < 2 || i >= nzp - 2 || j < 2 || j >= nxp - 2) return 0.f;
+      const int vz = min(max(i - pad, 0), P.nz - 1), vx = min(max(j - pad, 0), P.nx - 1);
+      return -2.f * G[static_cast<size_t>(i) * nxp + j] / v[vz * P.nx + vx];
+    };
+    const int i = pad + z, j = pad + x;
+    float val = at(i, j);
+    const int zi0 = z == 0 ? 0 : (z == P.nz - 1 ? pad + P.nz : -1), zi1 = z == 0 ? pad : nzp;
+    const int xj0 = x == 0 ? 0 : (x == P.nx - 1 ? pad + P.nx : -1), xj1 = x == 0 ? pad : nxp;
+    if (zi0 >= 0)
+      for (int ii = zi0; ii < zi1; ++ii) val += at(ii, j);
+    if (xj0 >= 0)
+      for (int jj = xj0; jj < xj1; ++jj) val += at(i, jj);
+    if (zi0 >= 0 && xj0 >= 0)
+      for (int ii = zi0; ii < zi1; ++ii)
+        for (int jj = xj0; jj < xj1; ++jj) val += at(ii, jj);
+    if (z == P.src_row && x == P.shot_cols[s]) {   // source-strength derivative (gpu.py:182,187)
+      const double vs = v[P.src_row * P.nx + x];
+      const double dz = layer_depth(i, nzp, pad), dxl = layer_depth(j, nxp, pad);
+      const float Ad = static_cast<float>(1.0 / (1.0 + P.damp_k * (dz * dz + dxl * dxl)));
+      const float c2 = static_cast<float>(vs * vs * P.dtdx2);
+      const float sigma = (c2 * Ad) / 12.f;
+      const float deriv = static_cast<float>(2.0 * vs / (P.amp_ref * P.amp_ref));
+      val += src_acc[solve] * deriv / sigma;
+    }
+    grad[idx] = val;
+    illum[idx] = illum_acc[idx] * (1.f / 144.f);
+  }
+}
+
 // FP32 throughput probe: 8 independent FMA chains per thread, scalar or
 // packed FP32x2, for the roofline denominator of the stencil kernels.
 template <bool PACKED>
@@ -970,6 +1102,7 @@ SolveFn kernel_for(int mode, bool fast) {
   switch (mode) {
     case SS_MODE_FORWARD: return fast ? solve_kernel<SS_MODE_FORWARD, true> : solve_kernel<SS_MODE_FORWARD, false>;
     case SS_MODE_GRADIENT: return fast ? solve_kernel<SS_MODE_GRADIENT, true> : solve_kernel<SS_MODE_GRADIENT, false>;
+    case SS_MODE_SEGMENT: return fast ? solve_kernel<SS_MODE_SEGMENT, true> : solve_kernel<SS_MODE_SEGMENT, false>;
     default: return fast ? solve_kernel<SS_MODE_IMAGES, true> : solve_kernel<SS_MODE_IMAGES, false>;
   }
 }
@@ -1046,14 +1179,15 @@ struct WsLayout {
   size_t err, hist, trace, gpad, grad, total;
 };
 
-WsLayout ws_layout(const ss_geometry* g, const Plan& p, int mode) {
+WsLayout ws_layout(const ss_geometry* g, const Plan& p, int mode, int hist_steps = -1) {
+  if (hist_steps < 0) hist_steps = g->nt;
   WsLayout w{};
   size_t off = 0;
   w.err = off;
   off = align_up(off + 256);
   if (mode != SS_MODE_FORWARD) {
     w.hist = off;
-    off = align_up(off + static_cast<size_t>(p.slots) * g->nt * p.C * p.bh * p.sw * sizeof(float));
+    off = align_up(off + static_cast<size_t>(p.slots) * hist_steps * p.C * p.bh * p.sw * sizeof(float));
     w.trace = off;
     off = align_up(off + static_cast<size_t>(p.slots) * g->nt * ((g->nx + 3) & ~3) * sizeof(float));
     w.gpad = off;
@@ -1091,6 +1225,7 @@ KParams base_params(const ss_geometry* g, const Plan& p, int n_models) {
   k.nact = p.ncg * p.nseg;
   k.nxs = (g->nx + 3) & ~3;
   k.n_solves = n_models * g->n_shots;
+  k.hist_steps = g->nt;
   return k;
 }
 
@@ -1382,6 +1517,78 @@ int32_t ss_images_noalloc(const ss_geometry* geom, int32_t n_models, const float
   SS_CUDA(cudaStreamSynchronize(st));
   if (flag == SS_ERR_NONFINITE) return fail(flag, "observations must be finite");
   if (flag != 0) return fail(flag, "a device-side bounded wait ran out (history copy did not complete)");
+  return SS_OK;
+}
+
+size_t ss_segment_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t ckpt_interval) {
+  if (check_geometry(geom) || n_models < 1 || ckpt_interval < 1) return 0;
+  Plan p;
+  if (make_plan(geom, SS_MODE_SEGMENT, n_models * geom->n_shots, &p)) return 0;
+  return ws_layout(geom, p, SS_MODE_SEGMENT, std::min(ckpt_interval, geom->nt)).total;
+}
+
+int32_t ss_adjoint_segment(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                           const float* ckpt, int32_t ckpt_interval, int32_t seg_index, const float* res,
+                           float* theta, float* gacc, float* illum_acc, float* src_acc, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (n_models < 1 || ckpt_interval < 1) return fail(SS_ERR_INVALID, "n_models and ckpt_interval must be positive");
+  const int n_ck = (geom->nt + ckpt_interval - 1) / ckpt_interval;
+  if (seg_index < 0 || seg_index >= n_ck) return fail(SS_ERR_INVALID, "segment index outside the checkpoints");
+  if (!vel || !wavelet || !ckpt || !res || !theta || !gacc || !illum_acc || !src_acc)
+    return fail(SS_ERR_INVALID, "every array argument is required");
+  Plan p;
+  rc = make_plan(geom, SS_MODE_SEGMENT, n_models * geom->n_shots, &p);
+  if (rc) return rc;
+  const int K = std::min(ckpt_interval, geom->nt);
+  const WsLayout L = ws_layout(geom, p, SS_MODE_SEGMENT, K);
+  if (!workspace || workspace_bytes < L.total) return fail(SS_ERR_WORKSPACE, "workspace missing or too small");
+  unsigned char* w = static_cast<unsigned char*>(workspace);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SS_CUDA(cudaMemsetAsync(w + L.err, 0, 256, st));
+  KParams k = base_params(geom, p, n_models);
+  k.vel = vel;
+  k.wav = wavelet;
+  k.trace = reinterpret_cast<float*>(w + L.trace);
+  k.gpad = reinterpret_cast<float*>(w + L.gpad);
+  k.grad = reinterpret_cast<float*>(w + L.grad);
+  k.grad_per_slot = 1;
+  k.hist = reinterpret_cast<float*>(w + L.hist);
+  k.hist_steps = K;
+  k.err = reinterpret_cast<int*>(w + L.err);
+  k.ckpt = const_cast<float*>(ckpt);
+  k.ckpt_interval = ckpt_interval;
+  k.n_ckpt = n_ck;
+  k.seg_index = seg_index;
+  k.seg_start = seg_index * ckpt_interval;
+  k.seg_steps = std::min(ckpt_interval, geom->nt - k.seg_start);
+  k.theta = theta;
+  k.gacc = gacc;
+  k.illum_acc = illum_acc;
+  k.src_acc_io = src_acc;
+  k.res_in = res;
+  k.eps = 1.f;
+  return launch(p, SS_MODE_SEGMENT, k, st);
+}
+
+int32_t ss_gradient_finish(const ss_geometry* geom, int32_t n_models, const float* vel, const float* gacc,
+                           const float* src_acc, const float* illum_acc, float* grad, float* illum, void* stream) {
+  g_last_error.clear();
+  int rc = check_geometry(geom);
+  if (rc) return rc;
+  if (n_models < 1 || !vel || !gacc || !src_acc || !illum_acc || !grad || !illum)
+    return fail(SS_ERR_INVALID, "bad arguments");
+  Plan p{};
+  p.nzp = geom->nz + 2 * geom->pad;
+  p.nxp = geom->nx + 2 * geom->pad;
+  KParams k = base_params(geom, p, n_models);
+  k.vel = vel;
+  const long long total = static_cast<long long>(n_models) * geom->n_shots * geom->nz * geom->nx;
+  finish_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(k, gacc, src_acc, illum_acc, grad,
+                                                                              illum);
+  SS_CUDA(cudaGetLastError());
   return SS_OK;
 }
 

@@ -147,6 +147,52 @@ class Engine:
                                         self._stream()), 'ss_images')
         return (img, illum, grad) if want_grad else (img, illum)
 
+    # -- checkpointed adjoint (differentiation) --------------------------------
+    def segment_workspace(self, n_models, interval):
+        with torch.cuda.device(self.device):
+            need = self.L.ss_segment_workspace_bytes(ctypes.byref(self.g), n_models, int(interval))
+        if need == 0:
+            _lib.check(_lib.ERR_UNSUPPORTED, 'ss_segment_workspace_bytes')
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = None
+            self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def adjoint_from_checkpoints(self, vel, wavelet, ckpt, interval, res):
+        """Per-shot gradient and illumination from forward checkpoints and an adjoint source.
+
+        ckpt [B, S, n_ck, 2, nzp, nxp] from forward(..., ckpt_interval=interval);
+        res [B, S, nt, nx] = dJ/d(gathers).  Segments run last-first, each
+        recomputing `interval` steps from its checkpoint (gpu.py:169-184).
+        """
+        g = self.g
+        B = vel.shape[0]
+        vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
+        wavelet = self._check_in(wavelet, (g.nt,), 'wavelet')
+        res = self._check_in(res, (B, g.n_shots, g.nt, g.nx), 'res')
+        n_ck = math.ceil(g.nt / interval)
+        if tuple(ckpt.shape) != (B, g.n_shots, n_ck, 2, *self.padded):
+            raise ValueError('checkpoints do not match the geometry and interval')
+        f32 = dict(dtype=torch.float32, device=self.device)
+        theta = torch.zeros(B, g.n_shots, 2, *self.padded, **f32)
+        gacc = torch.zeros(B, g.n_shots, *self.padded, **f32)
+        illum_acc = torch.zeros(B, g.n_shots, g.nz, g.nx, **f32)
+        src_acc = torch.zeros(B, g.n_shots, **f32)
+        ws = self.segment_workspace(B, interval)
+        with torch.cuda.device(self.device):
+            for k in range(n_ck - 1, -1, -1):
+                _lib.check(self.L.ss_adjoint_segment(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet),
+                                                     _lib.ptr(ckpt), int(interval), k, _lib.ptr(res), _lib.ptr(theta),
+                                                     _lib.ptr(gacc), _lib.ptr(illum_acc), _lib.ptr(src_acc),
+                                                     _lib.ptr(ws), ws.numel(), self._stream()), 'ss_adjoint_segment')
+            grad = torch.empty(B, g.n_shots, g.nz, g.nx, **f32)
+            illum = torch.empty_like(grad)
+            _lib.check(self.L.ss_gradient_finish(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(gacc), _lib.ptr(src_acc),
+                                                 _lib.ptr(illum_acc), _lib.ptr(grad), _lib.ptr(illum), self._stream()),
+                       'ss_gradient_finish')
+        self.status()
+        return grad, illum
+
     def mute_weights(self, v_mute, t_mute=0.12):
         g = self.g
         v_mute = self._check_in(v_mute, (v_mute.shape[0],), 'v_mute')
