@@ -23,6 +23,12 @@ cpu_baseline  the oracle's float32 restatement of the reference CPU path
 
 With torchrun, every rank simulates its own 500 models (weak scaling); the
 ranks exchange nothing on the data path.
+
+--workload uneven: the uneven batch instead: 2000 seeded (model, background,
+shot) solves on grids of 70-200 x 70-300 cells, 1000-3000 steps, 1-9 shots and
+1-3 backgrounds per model, planned into size classes, cluster sizes from the
+autotuner, replayed as one CUDA graph per step (shot-images/s and padded
+cell-steps/s; no CPU arm, the reference runs one fixed geometry only).
 """
 from __future__ import annotations
 
@@ -60,6 +66,10 @@ def parse():
     ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
     ap.add_argument('--models', type=int, default=N_MODELS, help='velocity models per GPU')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--workload', choices=('openfwi', 'uneven'), default='openfwi')
+    ap.add_argument('--solves', type=int, default=2000, help='uneven workload: solves per GPU')
+    ap.add_argument('--schedule', type=int, default=-1, choices=(-1, 0, 1, 2),
+                    help='uneven workload: stream schedule (-1: autotuned)')
     return ap.parse_args()
 
 
@@ -322,12 +332,119 @@ def run_ours(args):
     return 0
 
 
+def bus_id(dev):
+    import torch
+    props = torch.cuda.get_device_properties(dev)
+    if hasattr(props, 'pci_bus_id'):
+        return f'{getattr(props, "pci_domain_id", 0):08X}:{props.pci_bus_id:02X}:{getattr(props, "pci_device_id", 0):02X}.0'
+    return None
+
+
+def run_uneven(args):
+    """Uneven batch: forward of the true models, then RTM images of every (model, background) in one graph."""
+    import torch
+    from shotsweep_b200 import autotune, synth
+    from shotsweep_b200 import dist as D
+    from shotsweep_b200.batch import Shape, UnevenBatch
+    rank, world, local = D.init('nccl' if args.gpus > 1 else 'gloo', timeout_s=600)
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    wl = synth.uneven_workload(args.solves, seed=2 + rank)
+    max_nt = max(m['nt'] for m in wl)
+    t = np.arange(max_nt) * 1e-3
+    a = (np.pi * 15.0 * (t - 1.2 / 15.0)) ** 2
+    wav = torch.tensor((1 - 2 * a) * np.exp(-a) * 1e3, dtype=torch.float32, device=dev)
+    fb = UnevenBatch([Shape(m['truth'].shape[0], m['truth'].shape[1], m['nt'], m['shot_cols']) for m in wl], device=dev)
+    gathers = fb.forward(fb.pack_models([m['truth'] for m in wl]), wav)
+    shapes, bgs, obs_parts = [], [], []
+    for i, m in enumerate(wl):
+        nz, nx = m['truth'].shape
+        for bg in m['backgrounds']:
+            shapes.append(Shape(nz, nx, m['nt'], m['shot_cols'], v_mute=m['v_s']))
+            bgs.append(bg)
+            obs_parts.append(fb.unpack_traces(gathers, i).reshape(-1))
+    obs = torch.cat(obs_parts).contiguous()
+    del obs_parts, gathers
+    n_solves = sum(s.n_shots for s in shapes)
+    cell_steps = sum(s.cell_steps() for s in shapes)
+    table = autotune.tune(shapes, device=dev)
+    schedule = autotune.tune_schedule(shapes, table, device=dev) if args.schedule < 0 else args.schedule
+    ib = UnevenBatch(shapes, device=dev, clusters=table, schedule=schedule)
+    vb = ib.pack_models(bgs)
+    graph, img, illum = ib.capture_images(vb, wav, obs)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    ib.status()
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    D.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(bus_id(dev)) as clk:
+        for e0, e1 in events:
+            e0.record()
+            graph.replay()
+            e1.record()
+        torch.cuda.synchronize()
+    D.barrier()
+    ib.status()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in events]
+    total_ms = D.reduce(sum(step_ms), 'max', dev if world > 1 else None)
+    value = world * n_solves * args.steps / (total_ms * 1e-3)
+    # end to end: pinned host gathers copied in, images and illumination copied out, every step
+    obs_host = obs.cpu().pin_memory()
+    img_host = torch.empty(img.shape, dtype=img.dtype, pin_memory=True)
+    illum_host = torch.empty_like(img_host)
+    D.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        obs.copy_(obs_host, non_blocking=True)
+        graph.replay()
+        img_host.copy_(img, non_blocking=True)
+        illum_host.copy_(illum, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = D.reduce(e0.elapsed_time(e1), 'max', dev if world > 1 else None)
+    e2e = world * n_solves * args.steps / (e2e_ms * 1e-3)
+    peak = fp32_peak(dev)
+    achieved = cell_steps * 36 / (statistics.mean(step_ms) * 1e-3) / 1e12
+    classes = ib.classes()
+    if rank == 0:
+        print(json.dumps({
+            'metric': 'RTM shot-images/s (uneven batch: 70-200 x 70-300 cells, 1000-3000 steps, 1-9 shots)',
+            'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': total_ms / args.steps, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32', 'data': 'synthetic: seeded models of uneven size, gathers simulated from the true models',
+            'cell_steps_per_s': world * cell_steps * args.steps / (total_ms * 1e-3),
+            'config': {'workload': f'{n_solves} solves per GPU from {len(wl)} models ({len(shapes)} background rows), '
+                                   'one CUDA graph per step', 'solves_per_gpu': n_solves,
+                       'padded_cell_steps_per_gpu': cell_steps,
+                       'l2': f'inputs larger than L2 ({obs.numel() * 4 / 1e9:.1f} GB of gathers per step per GPU)',
+                       'autotune': {str(k): v for k, v in sorted(table.items())}, 'schedule': schedule,
+                       'classes': [{k: c[k] for k in ('min_cluster', 'cluster', 'n_solves', 'threads', 'slots',
+                                                      'stream')} for c in classes]},
+            'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
+                         'frac': achieved / peak, 'traffic': None,
+                         'algorithmic': '36 flops per padded cell per step (16 forward + 20 adjoint) over every solve'},
+            'cpu_baseline': None,
+            'e2e': {'value': e2e, 'unit': UNIT, 'h2d_bytes_per_step': obs.numel() * 4,
+                    'd2h_bytes_per_step': img.numel() * 8,
+                    'api': 'UnevenBatch graph replay with pinned host gathers in, images and illumination out'},
+            'clocks': clk.summary(), 'gpu_launches': len(classes) * args.steps,
+        }), flush=True)
+    del graph
+    D.finish()
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 0 or args.steps < 1:
         raise SystemExit('--steps must be positive and --warmup non-negative')
     if args.impl == 'reference':
         return run_reference(args)
+    if args.workload == 'uneven':
+        return run_uneven(args)
     return run_ours(args)
 
 

@@ -203,6 +203,76 @@ int32_t ss_images_noalloc(const ss_geometry* geom, int32_t n_models, const float
  * caller times the launch on `stream`; `out` must hold one float. */
 int32_t ss_fp32_probe(float* out, int32_t blocks, int32_t iters, int32_t packed, double* flops, void* stream);
 
+/* ---- Uneven batches ------------------------------------------------------
+ * Models of different grid size, step count and shot count in one launch
+ * sequence.  No counterpart in the reference, whose Sim is fixed to one
+ * 70x70 grid, 1000 steps and 5 shots (gpu.py:59,95-96,103,126-128); each
+ * solve computes exactly what ss_forward / ss_gradient / ss_images compute
+ * for a batch holding only its own geometry.
+ *
+ * Solves are grouped into size classes: a class holds the solves whose
+ * smallest fitting cluster (CTAs per solve) is the same, and runs as one
+ * persistent launch whose clusters take solves longest-first.  `concurrent`
+ * picks the streams: 0 runs the classes one after another on the caller's
+ * stream (heaviest first); 1 alternates them between the caller's stream and
+ * a second stream of the library, so that one class's tail overlaps the next
+ * class's start; 2 puts the classes whose clusters leave many SMs idle (large
+ * clusters pack the GPU's processing clusters badly) first on the caller's
+ * stream and runs the others beside them on the second stream, filling those
+ * SMs (falls back to 1 when the classes do not split).
+ *
+ * 1. ss_batch_plan (host): validates the items, forms the classes and the
+ *    per-class launch shapes (cluster size from `cluster_by_class`, indexed by
+ *    a class's smallest cluster, 0 or NULL = that smallest cluster; an
+ *    autotuner fills it), and writes a self-contained plan of *plan_bytes
+ *    bytes into `plan` (host memory; NULL: only report the sizes).
+ * 2. The caller copies the plan bytes unchanged to device memory.
+ * 3. ss_batch_run (stream-ordered): runs every class; the same plan serves
+ *    any number of runs with new data in the same layout. */
+#define SS_MAX_CLUSTER 16
+
+typedef struct ss_batch_item {          /* one velocity model (one background row) */
+    int32_t nz, nx, nt, pad;
+    int32_t n_shots, src_row;
+    int32_t shot_cols[SS_MAX_SHOTS];
+    int64_t vel_offset;   /* floats into vel: the model [nz][nx]                           */
+    int64_t obs_offset;   /* floats into obs (gradient, images) or gathers (forward):
+                             [n_shots][nt][nx]                                             */
+    int64_t out_offset;   /* floats into img / illum / grad: [n_shots][nz][nx]             */
+    float v_mute;         /* direct-wave mute velocity in m/s (gpu.py:142-150); <= 0: none */
+    int32_t reserved;
+} ss_batch_item;
+
+typedef struct ss_physics {             /* shared by every item (constants.py, gpu.py:77-96) */
+    double dx, dt, r_coef, vmax_damping, amp_ref;
+} ss_physics;
+
+typedef struct ss_batch_class_info {
+    int32_t min_cluster;  /* the size class: smallest cluster fitting its solves */
+    int32_t cluster;      /* CTAs per solve used                                 */
+    int32_t n_solves;
+    int32_t threads;      /* per CTA                                             */
+    int32_t smem_bytes;   /* per CTA                                             */
+    int32_t slots;        /* persistent clusters launched                        */
+    int32_t stream;       /* 0: the caller's stream, 1: the library's second one */
+    int32_t reserved;
+    double cell_steps;    /* sum over its solves of padded cells x steps         */
+} ss_batch_class_info;
+
+int32_t ss_batch_plan(const ss_physics* phys, int32_t mode, const ss_batch_item* items, int32_t n_items,
+                      const int32_t* cluster_by_class, int32_t concurrent, void* plan, size_t* plan_bytes,
+                      size_t* workspace_bytes);
+/* Smallest cluster (CTAs per solve) that fits the item in `mode`: its size
+ * class; negative ss_status if none does. */
+int32_t ss_batch_min_cluster(const ss_batch_item* item, int32_t mode);
+int32_t ss_batch_classes(const void* plan, ss_batch_class_info* out, int32_t max_classes, int32_t* n_classes);
+/* wavelet: at least the batch's largest nt samples (scaled as for ss_forward).
+ * gathers: forward mode output; img: images mode output; grad: gradient mode
+ * output, optional in images mode; illum: gradient and images modes. */
+int32_t ss_batch_run(const void* plan, const void* plan_device, const float* vel, const float* wavelet,
+                     const float* obs, float t_mute, float eps, int32_t laplacian, float* gathers, float* img,
+                     float* illum, float* grad, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -40,6 +40,30 @@ def make_geometry(nz, nx, nt, pad, shot_cols, src_row=1, dx=10.0, dt=1e-3, r_coe
     return g
 
 
+class BatchItem(ctypes.Structure):
+    """Mirror of ss_batch_item."""
+    _fields_ = [('nz', ctypes.c_int32), ('nx', ctypes.c_int32), ('nt', ctypes.c_int32), ('pad', ctypes.c_int32),
+                ('n_shots', ctypes.c_int32), ('src_row', ctypes.c_int32),
+                ('shot_cols', ctypes.c_int32 * MAX_SHOTS),
+                ('vel_offset', ctypes.c_int64), ('obs_offset', ctypes.c_int64), ('out_offset', ctypes.c_int64),
+                ('v_mute', ctypes.c_float), ('reserved', ctypes.c_int32)]
+
+
+class Physics(ctypes.Structure):
+    """Mirror of ss_physics."""
+    _fields_ = [('dx', ctypes.c_double), ('dt', ctypes.c_double), ('r_coef', ctypes.c_double),
+                ('vmax_damping', ctypes.c_double), ('amp_ref', ctypes.c_double)]
+
+
+class BatchClassInfo(ctypes.Structure):
+    """Mirror of ss_batch_class_info."""
+    _fields_ = [('min_cluster', ctypes.c_int32), ('cluster', ctypes.c_int32), ('n_solves', ctypes.c_int32),
+                ('threads', ctypes.c_int32), ('smem_bytes', ctypes.c_int32), ('slots', ctypes.c_int32),
+                ('stream', ctypes.c_int32), ('reserved', ctypes.c_int32), ('cell_steps', ctypes.c_double)]
+
+
+MAX_CLUSTER = 16
+
 _P = ctypes.c_void_p
 _SIGNATURES = {
     'ss_version': (ctypes.c_char_p, []),
@@ -70,6 +94,14 @@ _SIGNATURES = {
     'ss_adjoint_segment': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, ctypes.c_int32,
                                             ctypes.c_int32, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]),
     'ss_gradient_finish': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P]),
+    'ss_batch_plan': (ctypes.c_int32, [ctypes.POINTER(Physics), ctypes.c_int32, ctypes.POINTER(BatchItem),
+                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P,
+                                       ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
+    'ss_batch_min_cluster': (ctypes.c_int32, [ctypes.POINTER(BatchItem), ctypes.c_int32]),
+    'ss_batch_classes': (ctypes.c_int32, [_P, ctypes.POINTER(BatchClassInfo), ctypes.c_int32,
+                                          ctypes.POINTER(ctypes.c_int32)]),
+    'ss_batch_run': (ctypes.c_int32, [_P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_int32, _P, _P, _P,
+                                      _P, _P, ctypes.c_size_t, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

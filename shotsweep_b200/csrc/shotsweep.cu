@@ -34,6 +34,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/shotsweep.h"
 
@@ -95,6 +96,9 @@ __device__ __forceinline__ void st_cluster_v4(uint32_t addr, float4 v) {
   asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
                "f"(v.w)
                : "memory");
+}
+__device__ __forceinline__ void st_cluster_u32(uint32_t addr, int v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -167,6 +171,26 @@ __device__ __forceinline__ double layer_depth(int i, int n, int pad) {
 // ----------------------------------------------------------------------------
 // Fused per-solve kernel
 // ----------------------------------------------------------------------------
+// One model (one background row) of an uneven batch, as the kernel reads it:
+// its grid, its band plan for the launch's cluster size, and where its data
+// lie in the packed arrays.  Built on the host by the batch planner.
+struct BatchItemDev {
+  int nz, nx, nt, pad, nzp, nxp, src_row, n_shots;
+  int ncg, nseg, bh, nact;            // column groups, tile rows per band, band rows, active threads
+  int shot_cols[SS_MAX_SHOTS];
+  long long vel_off;                  // floats: [nz][nx] velocities
+  long long obs_off;                  // floats: [n_shots][nt][nx] observations (images) or gathers (forward)
+  long long out_off;                  // floats: [n_shots][nz][nx] img / illum / grad
+  double damp_k;                      // damping constant of this pad
+  float vmute;                        // mute velocity; <= 0: no mute
+  int reserved;
+};
+
+// The current solve's geometry inside a batch launch (registers).
+struct SolveGeo {
+  int nz, nx, nt, pad, nzp, nxp, src_row, ncg, nseg, bh, nact, rs, sw;
+};
+
 struct KParams {
   int nz, nx, nt, pad, nzp, nxp, n_shots, src_row;
   int shot_cols[SS_MAX_SHOTS];
@@ -200,6 +224,11 @@ struct KParams {
   float* illum_acc;    // [solve][nz][nx]: += sum_t S^2 over the segment
   float* src_acc_io;   // [solve]: += sum_t th(source cell) * w[t]
   const float* res_in; // [solve][nt][nx]: adjoint source (the gathers' cotangent)
+  // uneven batch: per-item geometry, the longest-first solve list, its counter
+  const BatchItemDev* items;
+  const int* order;    // [n_solves] item << 4 | shot
+  int* counter;        // next entry of order; zero at launch
+  size_t hist_slot, trace_slot, gpad_slot, grad_slot;   // per-slot scratch (floats)
 };
 
 struct Smem {
@@ -226,37 +255,36 @@ __device__ __forceinline__ float mute_weight(int t, int r, int shot_col, float d
 // for images, normalise by illumination and Laplacian-filter (gpu.py:206-209).
 // Called by every thread of the cluster; gp holds this slot's padded gradient.
 template <int MODE>
-__device__ __forceinline__ void epilogue(const KParams& P, Smem& S, float* gp, int solve, int slot, int rank, int tid,
-                                         int nthr) {
+__device__ __forceinline__ void epilogue(const KParams& P, Smem& S, float* gp, float* go, const float* il, float* im,
+                                         const int nz, const int nx, const int pad, const int nzp, const int nxp,
+                                         int rank, int tid, int nthr) {
     // ---- fold the padding onto the edge cells (gpu.py:56-67, 185-187) ----
-    float* go = P.grad_per_slot ? P.grad + static_cast<size_t>(slot) * P.nz * P.nx
-                                : P.grad + static_cast<size_t>(solve) * P.nz * P.nx;
     {
-      const int zlo = 2, zhi = P.nzp - 2, xlo = 2, xhi = P.nxp - 2;
-      auto G = [&](int i, int j) -> float { return gp[static_cast<size_t>(i) * P.nxp + j]; };
+      const int zlo = 2, zhi = nzp - 2, xlo = 2, xhi = nxp - 2;
+      auto G = [&](int i, int j) -> float { return gp[static_cast<size_t>(i) * nxp + j]; };
       const int gthr = rank * nthr + tid, gstride = P.C * nthr;
-      for (int o = gthr; o < P.nz * P.nx; o += gstride) {
-        const int z = o / P.nx, x = o - z * P.nx;
-        const bool zc = (z == 0 || z == P.nz - 1), xc = (x == 0 || x == P.nx - 1);
+      for (int o = gthr; o < nz * nx; o += gstride) {
+        const int z = o / nx, x = o - z * nx;
+        const bool zc = (z == 0 || z == nz - 1), xc = (x == 0 || x == nx - 1);
         if (zc && xc) continue;   // corners: one warp each below
-        const int i = P.pad + z, j = P.pad + x;
+        const int i = pad + z, j = pad + x;
         float val = G(i, j);
         if (z == 0)
-          for (int ii = zlo; ii < P.pad; ++ii) val += G(ii, j);
-        if (z == P.nz - 1)
-          for (int ii = P.pad + P.nz; ii < zhi; ++ii) val += G(ii, j);
+          for (int ii = zlo; ii < pad; ++ii) val += G(ii, j);
+        if (z == nz - 1)
+          for (int ii = pad + nz; ii < zhi; ++ii) val += G(ii, j);
         if (x == 0)
-          for (int jj = xlo; jj < P.pad; ++jj) val += G(i, jj);
-        if (x == P.nx - 1)
-          for (int jj = P.pad + P.nx; jj < xhi; ++jj) val += G(i, jj);
+          for (int jj = xlo; jj < pad; ++jj) val += G(i, jj);
+        if (x == nx - 1)
+          for (int jj = pad + nx; jj < xhi; ++jj) val += G(i, jj);
         go[o] = val;
       }
       const int warp = tid >> 5, lane = tid & 31, n_warps = nthr >> 5;
       for (int corner = warp; rank == 0 && corner < 4; corner += n_warps) {
-        const int z = (corner & 1) ? P.nz - 1 : 0, x = (corner & 2) ? P.nx - 1 : 0;
-        const int i = P.pad + z, j = P.pad + x;
-        const int i0 = z == 0 ? zlo : P.pad + P.nz, i1 = z == 0 ? P.pad : zhi;
-        const int j0 = x == 0 ? xlo : P.pad + P.nx, j1 = x == 0 ? P.pad : xhi;
+        const int z = (corner & 1) ? nz - 1 : 0, x = (corner & 2) ? nx - 1 : 0;
+        const int i = pad + z, j = pad + x;
+        const int i0 = z == 0 ? zlo : pad + nz, i1 = z == 0 ? pad : zhi;
+        const int j0 = x == 0 ? xlo : pad + nx, j1 = x == 0 ? pad : xhi;
         float val = 0.f;
         for (int ii = i0 + lane; ii < i1; ii += 32) val += G(ii, j);   // strip above/below
         for (int jj = j0 + lane; jj < j1; jj += 32) val += G(i, jj);   // strip left/right
@@ -264,16 +292,15 @@ __device__ __forceinline__ void epilogue(const KParams& P, Smem& S, float* gp, i
         for (int q = lane; q < bn; q += 32) val += G(i0 + q / bw, j0 + q % bw);   // corner block
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) val += __shfl_xor_sync(0xffffffffu, val, off);
-        if (lane == 0) go[z * P.nx + x] = G(i, j) + val;
+        if (lane == 0) go[z * nx + x] = G(i, j) + val;
       }
     }
     if (MODE == SS_MODE_IMAGES) {
       __threadfence();
       cluster_sync();
       // ---- image epilogue (gpu.py:206-209) --------------------------------
-      const float* il = P.illum + static_cast<size_t>(solve) * P.nz * P.nx;
       float mx = -INFINITY;
-      for (int o = tid; o < P.nz * P.nx; o += nthr) mx = fmaxf(mx, il[o]);
+      for (int o = tid; o < nz * nx; o += nthr) mx = fmaxf(mx, il[o]);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
       if ((tid & 31) == 0) S.red[tid >> 5] = mx;
@@ -288,20 +315,19 @@ __device__ __forceinline__ void epilogue(const KParams& P, Smem& S, float* gp, i
       const float emax = P.eps * S.red[0];
       float* pre = gp;   // reuse the padded-gradient scratch for the unfiltered image
       const int gthr = rank * nthr + tid, gstride = P.C * nthr;
-      for (int o = gthr; o < P.nz * P.nx; o += gstride) {
+      for (int o = gthr; o < nz * nx; o += gstride) {
         const float den = fmaxf(il[o] + emax, 1.17549435e-38f);
         pre[o] = -go[o] / den;
       }
-      float* im = P.img + static_cast<size_t>(solve) * P.nz * P.nx;
       if (P.laplacian) {
         __threadfence();
         cluster_sync();
-        for (int o = gthr; o < P.nz * P.nx; o += gstride) {
-          const int z = o / P.nx, x = o - z * P.nx;
+        for (int o = gthr; o < nz * nx; o += gstride) {
+          const int z = o / nx, x = o - z * nx;
           auto I = [&](int zz, int xx) -> float {
-            zz = min(max(zz, 0), P.nz - 1);
-            xx = min(max(xx, 0), P.nx - 1);
-            return pre[zz * P.nx + xx];
+            zz = min(max(zz, 0), nz - 1);
+            xx = min(max(xx, 0), nx - 1);
+            return pre[zz * nx + xx];
           };
           const float c = I(z, x);
           const float lz = -I(z - 2, x) + 16.f * I(z - 1, x) - 30.f * c + 16.f * I(z + 1, x) - I(z + 2, x);
@@ -309,7 +335,7 @@ __device__ __forceinline__ void epilogue(const KParams& P, Smem& S, float* gp, i
           im[o] = -((lz + lx) / 12.f);
         }
       } else {
-        for (int o = gthr; o < P.nz * P.nx; o += gstride) im[o] = pre[o];
+        for (int o = gthr; o < nz * nx; o += gstride) im[o] = pre[o];
       }
     }
 }
@@ -434,18 +460,28 @@ __device__ __forceinline__ void add_at(float4& v, int m, float a) {
 // neighbouring tiles read (the full field of the current level, ping-pong
 // buffered).  The time loop is unrolled by two so that the two register
 // arrays swap roles without moves.
-template <int MODE, bool FAST>
+template <int MODE, bool FAST, bool BATCH>
 __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) {
   constexpr int H = kRowsPerThread;
   constexpr bool ADJ = MODE != SS_MODE_FORWARD;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Geometry: compile-time constants on the fast path, parameter-bank reads
-  // otherwise (macros, so that the generic path keeps no registers for them).
-#define RS (FAST ? kFastRS : P.rs)      /* shared row stride (floats) */
-#define NX (FAST ? 70 : P.nx)           /* receivers per shot */
-#define PAD (FAST ? 40 : P.pad)
-#define SW (FAST ? kFastRS - 8 : P.sw)  /* history row width */
-#define NXS (FAST ? 72 : P.nxs)         /* padded trace row */
+  // on the generic path (macros, so that it keeps no registers for them), and
+  // the current solve's values in an uneven batch (BATCH).
+  SolveGeo gs{};
+#define RS (FAST ? kFastRS : BATCH ? gs.rs : P.rs)        /* shared row stride (floats) */
+#define NX (FAST ? 70 : BATCH ? gs.nx : P.nx)             /* receivers per shot */
+#define PAD (FAST ? 40 : BATCH ? gs.pad : P.pad)
+#define SW (FAST ? kFastRS - 8 : BATCH ? gs.sw : P.sw)    /* history row width */
+#define NXS (FAST ? 72 : P.nxs)                           /* padded trace row */
+#define GNZ (BATCH ? gs.nz : P.nz)
+#define GNT (BATCH ? gs.nt : P.nt)
+#define GNZP (BATCH ? gs.nzp : P.nzp)
+#define GNXP (BATCH ? gs.nxp : P.nxp)
+#define GBH (BATCH ? gs.bh : P.bh)
+#define GNCG (BATCH ? gs.ncg : P.ncg)
+#define GNSEG (BATCH ? gs.nseg : P.nseg)
+#define GNACT (BATCH ? gs.nact : P.nact)
 
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
@@ -456,20 +492,32 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   const int n_slots = static_cast<int>(gridDim.x / P.C);
 
   // ---- shared-memory carve-up (identical in every CTA of the cluster) ----
+  // Fixed geometry: fields, history slabs, then the rest.  Uneven batch:
+  // barriers, wavelet, reduction words and receiver rows first, at fixed
+  // offsets; the fields, slabs and zero tile of each solve after them.
   Smem S;
-  const size_t field_floats = static_cast<size_t>(P.bh + 4) * RS;
-  {
-    const size_t stage = ADJ ? static_cast<size_t>(P.bh) * SW : 0;
+  size_t field_floats = static_cast<size_t>(P.bh + 4) * RS;
+  size_t stage_floats = ADJ ? static_cast<size_t>(P.bh) * SW : 0;
+  float* solve_smem = nullptr;   // BATCH: start of the per-solve part
+  if (!BATCH) {
     float* base = reinterpret_cast<float*>(smem_raw);
     S.f[0] = base;
     S.f[1] = base + field_floats;
     S.stg0 = base + 2 * field_floats;
-    S.wav = base + 2 * field_floats + kStages * stage;
+    S.wav = base + 2 * field_floats + kStages * stage_floats;
     S.red = S.wav + ((P.nt + 31) & ~31);
     S.res0 = S.red + 32;
     S.trc = S.res0 + kStages * NXS;
     S.dummy = S.trc + kTraceRing * NXS;
     S.bar = reinterpret_cast<uint64_t*>(S.dummy + (H + 4) * RS + H * SW);   // [0,kStages) history, then 2 halos
+  } else {
+    S.bar = reinterpret_cast<uint64_t*>(smem_raw);
+    static_assert((kStages + 2) * sizeof(uint64_t) <= 16 * sizeof(float), "barriers overrun the wavelet");
+    S.wav = reinterpret_cast<float*>(smem_raw) + 16;   // 64-byte aligned after the barriers
+    S.red = S.wav + ((P.nt + 31) & ~31);
+    S.res0 = S.red + 32;
+    S.trc = S.res0 + kStages * NXS;
+    solve_smem = S.trc + kTraceRing * NXS;
   }
   for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
   if (tid == 0) {
@@ -478,71 +526,121 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   }
   const uint32_t hist_bar0 = smem_u32(&S.bar[0]);
   const uint32_t halo_bar0 = smem_u32(&S.bar[kStages]);
-  const size_t stage_floats = ADJ ? static_cast<size_t>(P.bh) * SW : 0;
   uint32_t hist_phase = 0, halo_phase = 0;   // parity of the next wait, one bit per buffer
   auto stage_buf = [&](int b) { return S.stg0 + b * stage_floats; };
   auto res_buf = [&](int b) { return S.res0 + b * NXS; };
+  int* const next_solve = reinterpret_cast<int*>(S.red) + 31;   // BATCH: the cluster's next entry of P.order
 
-  // ---- this thread's tile -------------------------------------------------
-  // Warp-aligned mapping: the first nseg*ncg_main threads cover column
-  // groups [0, ncg_main) with one tile row per warp; the remaining column
-  // groups of every tile row are packed after them.
-  const bool active = tid < P.nact;
-  const int ncg_main = (P.ncg / 32) * 32, ncg_rem = P.ncg - ncg_main;
-  int cg = 0, seg = 0;
-  if (active) {
-    if (tid < P.nseg * ncg_main) {
-      seg = tid / ncg_main;
-      cg = tid - seg * ncg_main;
-    } else {
-      const int u = tid - P.nseg * ncg_main;
-      seg = u / ncg_rem;
-      cg = ncg_main + (u - seg * ncg_rem);
-    }
-  }
-  const int row0 = 2 + rank * P.bh;               // first padded row of the band
-  const int myrow = row0 + seg * H;               // first padded row of this thread
-  const int col0 = 2 + 4 * cg;                    // first padded column
-  const int o0 = 4 * cg + 4;                      // shared-memory column offset of col0
-  const int lr0 = seg * H;                        // shared row of tile row -2
-  const int src_r = PAD + P.src_row;            // padded row of sources and receivers
-  const int rec_rank = (src_r - 2) / P.bh;
-
-  // Halo exchange: the two edge rows of a band are pushed into the
-  // neighbour's halo rows with st.async, which counts the bytes on the
-  // neighbour's halo mbarrier of that buffer; readers of halo rows wait on it.
-  const bool edge_up = active && seg == 0 && rank > 0;
-  const bool edge_dn = active && seg == P.nseg - 1 && rank < P.C - 1;
-  const uint32_t field_bytes = static_cast<uint32_t>(field_floats * sizeof(float));
-  const uint32_t up_addr = edge_up ? mapa(smem_u32(S.f[0] + (P.bh + 2) * RS + o0), rank - 1) : 0u;
-  const uint32_t up_bar = edge_up ? mapa(halo_bar0, rank - 1) : 0u;
-  const uint32_t dn_addr = edge_dn ? mapa(smem_u32(S.f[0] + o0), rank + 1) : 0u;
-  const uint32_t dn_bar = edge_dn ? mapa(halo_bar0, rank + 1) : 0u;
-  const uint32_t halo_bytes = 32u * P.ncg * ((rank > 0 ? 1u : 0u) + (rank < P.C - 1 ? 1u : 0u));
-  const int rec_k = (active && src_r >= myrow && src_r < myrow + H) ? src_r - myrow : -1;
-  // A warp with any tile on the lower band edge computes its rows bottom-up,
-  // so that the rows pushed to the next band are ready early in the step;
-  // the order is uniform per warp (the tile is in registers, any order works).
-  const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
-
-  const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(P.bh) * SW * sizeof(float));
-  const size_t hist_slot = static_cast<size_t>(P.hist_steps) * P.C * P.bh * SW;
   constexpr bool SEG = MODE == SS_MODE_SEGMENT;
-  const int lvl_lo = SEG ? P.seg_start : 0;                  // first level of the time range
-  const int n_steps = SEG ? P.seg_steps : P.nt;               // steps of each sweep
-  const int lvl_hi = lvl_lo + n_steps - 1;
-  float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * P.bh * SW
-                               : nullptr;
-  const size_t hist_step = static_cast<size_t>(P.C) * P.bh * SW;
+  const size_t hist_step_fixed = static_cast<size_t>(P.C) * P.bh * SW;
+  const size_t trace_slot = BATCH ? P.trace_slot : static_cast<size_t>(P.nt) * NXS;
 
   cluster_sync();   // barriers initialised and wavelet staged everywhere
 
-  for (int solve = slot; solve < P.n_solves; solve += n_slots) {
-    const int b = solve / P.n_shots;
-    const int s = solve - b * P.n_shots;
-    const float* v = P.vel + static_cast<size_t>(b) * P.nz * NX;
-    const int shot_col = P.shot_cols[s];
+  for (int it = slot;; it += n_slots) {
+    // ---- next solve: round robin, or (uneven batch) the next entry of the
+    // longest-first list, taken by rank 0 and broadcast through DSMEM ------
+    int solve, b, s;
+    if (BATCH) {
+      if (rank == 0 && tid == 0) {
+        const int j = atomicAdd(P.counter, 1);
+        for (int r = 0; r < P.C; ++r) st_cluster_u32(mapa(smem_u32(next_solve), r), j);
+      }
+      cluster_sync();
+      const int j = *next_solve;
+      if (j >= P.n_solves) break;
+      solve = P.order[j];
+      b = solve >> 4;
+      s = solve & 15;
+      const BatchItemDev& item = P.items[b];
+      gs.nz = item.nz;
+      gs.nx = item.nx;
+      gs.nt = item.nt;
+      gs.pad = item.pad;
+      gs.nzp = item.nzp;
+      gs.nxp = item.nxp;
+      gs.src_row = item.src_row;
+      gs.ncg = item.ncg;
+      gs.nseg = item.nseg;
+      gs.bh = item.bh;
+      gs.nact = item.nact;
+      gs.rs = 4 * item.ncg + 8;
+      gs.sw = 4 * item.ncg;
+      // per-solve part of shared memory
+      field_floats = static_cast<size_t>(gs.bh + 4) * gs.rs;
+      stage_floats = ADJ ? static_cast<size_t>(gs.bh) * gs.sw : 0;
+      S.f[0] = solve_smem;
+      S.f[1] = solve_smem + field_floats;
+      S.stg0 = solve_smem + 2 * field_floats;
+      S.dummy = S.stg0 + kStages * stage_floats;
+    } else {
+      if (it >= P.n_solves) break;
+      solve = it;
+      b = solve / P.n_shots;
+      s = solve - b * P.n_shots;
+    }
+    const float* v = BATCH ? P.vel + P.items[b].vel_off : P.vel + static_cast<size_t>(b) * P.nz * NX;
+    const int shot_col = BATCH ? P.items[b].shot_cols[s] : P.shot_cols[s];
     const int src_c = PAD + shot_col;
+    // offsets of this solve's [nz][nx] outputs and [nt][nx] traces
+    const size_t out_off = BATCH ? static_cast<size_t>(P.items[b].out_off) + static_cast<size_t>(s) * GNZ * NX
+                                 : static_cast<size_t>(solve) * P.nz * NX;
+    const size_t trc_off = BATCH ? static_cast<size_t>(P.items[b].obs_off) + static_cast<size_t>(s) * GNT * NX
+                                 : static_cast<size_t>(solve) * P.nt * NX;
+    const double damp_k = BATCH ? P.items[b].damp_k : P.damp_k;
+    const float v_mute = BATCH ? P.items[b].vmute : (P.vmute ? P.vmute[b] : 0.f);
+    const bool muted = BATCH ? v_mute > 0.f : P.vmute != nullptr;
+
+    // ---- this thread's tile -----------------------------------------------
+    // Warp-aligned mapping: the first nseg*ncg_main threads cover column
+    // groups [0, ncg_main) with one tile row per warp; the remaining column
+    // groups of every tile row are packed after them.
+    const bool active = tid < GNACT;
+    const int ncg_main = (GNCG / 32) * 32, ncg_rem = GNCG - ncg_main;
+    int cg = 0, seg = 0;
+    if (active) {
+      if (tid < GNSEG * ncg_main) {
+        seg = tid / ncg_main;
+        cg = tid - seg * ncg_main;
+      } else {
+        const int u = tid - GNSEG * ncg_main;
+        seg = u / ncg_rem;
+        cg = ncg_main + (u - seg * ncg_rem);
+      }
+    }
+    const int row0 = 2 + rank * GBH;                // first padded row of the band
+    const int myrow = row0 + seg * H;               // first padded row of this thread
+    const int col0 = 2 + 4 * cg;                    // first padded column
+    const int o0 = 4 * cg + 4;                      // shared-memory column offset of col0
+    const int lr0 = seg * H;                        // shared row of tile row -2
+    const int src_r = PAD + (BATCH ? gs.src_row : P.src_row);   // padded row of sources and receivers
+    const int rec_rank = (src_r - 2) / GBH;
+
+    // Halo exchange: the two edge rows of a band are pushed into the
+    // neighbour's halo rows with st.async, which counts the bytes on the
+    // neighbour's halo mbarrier of that buffer; readers of halo rows wait on it.
+    const bool edge_up = active && seg == 0 && rank > 0;
+    const bool edge_dn = active && seg == GNSEG - 1 && rank < P.C - 1;
+    const uint32_t field_bytes = static_cast<uint32_t>(field_floats * sizeof(float));
+    const uint32_t up_addr = edge_up ? mapa(smem_u32(S.f[0] + (GBH + 2) * RS + o0), rank - 1) : 0u;
+    const uint32_t up_bar = edge_up ? mapa(halo_bar0, rank - 1) : 0u;
+    const uint32_t dn_addr = edge_dn ? mapa(smem_u32(S.f[0] + o0), rank + 1) : 0u;
+    const uint32_t dn_bar = edge_dn ? mapa(halo_bar0, rank + 1) : 0u;
+    const uint32_t halo_bytes = 32u * GNCG * ((rank > 0 ? 1u : 0u) + (rank < P.C - 1 ? 1u : 0u));
+    const int rec_k = (active && src_r >= myrow && src_r < myrow + H) ? src_r - myrow : -1;
+    // A warp with any tile on the lower band edge computes its rows bottom-up,
+    // so that the rows pushed to the next band are ready early in the step;
+    // the order is uniform per warp (the tile is in registers, any order works).
+    const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
+
+    const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(GBH) * SW * sizeof(float));
+    const size_t hist_slot = BATCH ? P.hist_slot : static_cast<size_t>(P.hist_steps) * hist_step_fixed;
+    const int lvl_lo = SEG ? P.seg_start : 0;                  // first level of the time range
+    const int n_steps = SEG ? P.seg_steps : GNT;                // steps of each sweep
+    const int lvl_hi = lvl_lo + n_steps - 1;
+    const size_t hist_step = BATCH ? static_cast<size_t>(P.C) * GBH * SW : hist_step_fixed;
+    float* const hist_mine = ADJ ? P.hist + static_cast<size_t>(slot) * hist_slot + static_cast<size_t>(rank) * GBH * SW
+                                 : nullptr;
 
     // ---- per-cell coefficients ----------------------------------------
     float2 kap[H][2], nsig[H][2], acc[H][2], A[H][2], B[H][2];
@@ -553,10 +651,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       for (int m = 0; m < 4; ++m) {
         const int r = myrow + k, c = col0 + m;
         float kv = 0.f, sv = 0.f;
-        if (active && r < P.nzp - 2 && c < P.nxp - 2) {
-          const double dz = layer_depth(r, P.nzp, PAD), dxl = layer_depth(c, P.nxp, PAD);
-          const float Ad = static_cast<float>(1.0 / (1.0 + P.damp_k * (dz * dz + dxl * dxl)));
-          const int vz = min(max(r - PAD, 0), P.nz - 1), vx = min(max(c - PAD, 0), NX - 1);
+        if (active && r < GNZP - 2 && c < GNXP - 2) {
+          const double dz = layer_depth(r, GNZP, PAD), dxl = layer_depth(c, GNXP, PAD);
+          const float Ad = static_cast<float>(1.0 / (1.0 + damp_k * (dz * dz + dxl * dxl)));
+          const int vz = min(max(r - PAD, 0), GNZ - 1), vx = min(max(c - PAD, 0), NX - 1);
           const double vp = v[vz * NX + vx];
           const float c2 = static_cast<float>(vp * vp * P.dtdx2);
           kv = 2.f * Ad;
@@ -581,14 +679,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     // run behind warp-uniform branches: only warps holding such cells pay.
     const bool warp_src = __any_sync(0xffffffffu, src_k >= 0);
     const bool warp_rec = __any_sync(0xffffffffu, rec_k >= 0);
-    const double v_src = v[P.src_row * NX + shot_col];
+    const double v_src = v[(src_r - PAD) * NX + shot_col];
     const float amp = static_cast<float>((v_src / P.amp_ref) * (v_src / P.amp_ref));
 
     const int tstride = (MODE == SS_MODE_FORWARD) ? NX : NXS;
     float src_acc = 0.f;   // sum_t th(source cell) * w[t]
     int flushed = 0;       // receiver rows below this level are in global memory
-    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + static_cast<size_t>(solve) * P.nt * NX
-                                             : P.trace + static_cast<size_t>(slot) * P.nt * NXS;
+    float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + trc_off : P.trace + static_cast<size_t>(slot) * trace_slot;
 
     // ---- zero both shared fields (own rows and halos) --------------------
     for (size_t i = tid; i < field_floats / 2; i += nthr) {
@@ -623,7 +720,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           if (res_here) bulk_load(smem_u32(res_buf(bn)), trace + static_cast<size_t>(tn) * NXS, res_bytes, bar);
         }
       }
-      if (MODE == SS_MODE_FORWARD && fwd && P.ckpt != nullptr && lvl % P.ckpt_interval == 0 && active) {
+      if (!BATCH && MODE == SS_MODE_FORWARD && fwd && P.ckpt != nullptr && lvl % P.ckpt_interval == 0 && active) {
         float* ck = P.ckpt + ((static_cast<size_t>(solve) * P.n_ckpt + lvl / P.ckpt_interval) * 2) * P.nzp * P.nxp;
 #pragma unroll
         for (int k = 0; k < H; ++k) {
@@ -641,8 +738,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       }
       if ((edge_up || edge_dn) && step > 0) {
         mbar_wait_bounded(halo_bar0 + 8u * cur, (halo_phase >> cur) & 1u, P.err);
-        halo_phase ^= 1u << cur;
+        if (!BATCH) halo_phase ^= 1u << cur;
       }
+      // A halo barrier completes one phase per step after the first.  In a
+      // batch the edge threads change from solve to solve, so every thread
+      // follows the phases, waiting or not.
+      if (BATCH && step > 0) halo_phase ^= 1u << cur;
       if (!fwd) {
         mbar_wait_bounded(hist_bar0 + 8u * bi, (hist_phase >> bi) & 1u, P.err);
         hist_phase ^= 1u << bi;
@@ -707,7 +808,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           flushed = hi + 1;
         };
         if (lvl - flushed == kTraceRing) flush(lvl - 1);
-        if (lvl == P.nt - 1) {   // the last level, recorded after the final barrier
+        if (lvl == GNT - 1) {   // the last level, recorded after the final barrier
           #pragma unroll 1
         for (int r = tid; r < NX; r += nthr)
             S.trc[(lvl % kTraceRing) * NXS + r] = Y[(src_r - row0 + 2) * RS + PAD + r + 2];
@@ -766,14 +867,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       fence_proxy_async_all();
     }
     {
-      float* il = P.illum + static_cast<size_t>(solve) * P.nz * NX;
+      float* il = P.illum + out_off;
 #pragma unroll
       for (int k = 0; k < H; ++k)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const int z = myrow + k - PAD, x = col0 + m - PAD;
           const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
-          if (active && z >= 0 && z < P.nz && x >= 0 && x < NX) {
+          if (active && z >= 0 && z < GNZ && x >= 0 && x < NX) {
             if (SEG)
               P.illum_acc[static_cast<size_t>(solve) * P.nz * NX + z * NX + x] += a;
             else
@@ -795,14 +896,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       fence_proxy_async_all();
       __syncthreads();
     } else if (rank == rec_rank) {
-      const float* ob = P.obs + static_cast<size_t>(solve) * P.nt * NX;
-      const float vm = P.vmute ? P.vmute[b] : 0.f;
-      for (int i = tid; i < P.nt * NX; i += nthr) {
+      const float* ob = P.obs + trc_off;
+      const float vm = v_mute;
+      for (int i = tid; i < GNT * NX; i += nthr) {
         const int t = i / NX, r = i - t * NX;
         const float o = ob[i];
         if (!isfinite(o)) atomicExch(P.err, static_cast<int>(SS_ERR_NONFINITE));
         float res = trace[t * NXS + r] - o;
-        if (P.vmute) res *= mute_weight(t, r, shot_col, P.dx, P.dt, vm, P.t_mute);
+        if (muted) res *= mute_weight(t, r, shot_col, P.dx, P.dt, vm, P.t_mute);
         trace[t * NXS + r] = res;
       }
       fence_proxy_async_all();   // these rows are read back by bulk copies
@@ -866,15 +967,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 
     // ---- padded gradient 2/v * sum_t th*S(p), plus the source term -------
     // acc holds -sum_t th*S (the history holds -S); nsig = -sigma.
-    float* gp = P.gpad + static_cast<size_t>(slot) * P.nzp * P.nxp;
+    float* gp = P.gpad + static_cast<size_t>(slot) * (BATCH ? P.gpad_slot : static_cast<size_t>(P.nzp) * P.nxp);
     if (active) {
 #pragma unroll
       for (int k = 0; k < H; ++k)
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
           const int r = myrow + k, c = col0 + m;
-          if (r < P.nzp - 2 && c < P.nxp - 2) {
-            const int vz = min(max(r - PAD, 0), P.nz - 1), vx = min(max(c - PAD, 0), NX - 1);
+          if (r < GNZP - 2 && c < GNXP - 2) {
+            const int vz = min(max(r - PAD, 0), GNZ - 1), vx = min(max(c - PAD, 0), NX - 1);
             const float vp = v[vz * NX + vx];
             const float a = (m & 1) ? acc[k][m >> 1].y : acc[k][m >> 1].x;
             float gval = -2.f * a / vp;
@@ -883,13 +984,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
               const float ns = (m & 1) ? nsig[k][m >> 1].y : nsig[k][m >> 1].x;
               gval += src_acc * deriv / -ns;
             }
-            gp[static_cast<size_t>(r) * P.nxp + c] = gval;
+            gp[static_cast<size_t>(r) * GNXP + c] = gval;
           }
         }
     }
     __threadfence();
     cluster_sync();
-    epilogue<MODE>(P, S, gp, solve, slot, rank, tid, nthr);
+    {
+      float* go = P.grad_per_slot ? P.grad + static_cast<size_t>(slot) * (BATCH ? P.grad_slot : static_cast<size_t>(P.nz) * P.nx)
+                                  : P.grad + out_off;
+      epilogue<MODE>(P, S, gp, go, P.illum + out_off, P.img + out_off, GNZ, NX, PAD, GNZP, GNXP, rank, tid, nthr);
+    }
     __threadfence();
     cluster_sync();   // scratch of this slot is free for the next solve
   }
@@ -901,6 +1006,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 #undef PAD
 #undef SW
 #undef NXS
+#undef GNZ
+#undef GNT
+#undef GNZP
+#undef GNXP
+#undef GBH
+#undef GNCG
+#undef GNSEG
+#undef GNACT
 
 // ----------------------------------------------------------------------------
 // Small helper kernels (module-level functions of the reference)
@@ -1100,10 +1213,22 @@ bool fast_geometry(int nx, int pad) { return nx == 70 && pad == 40; }
 
 SolveFn kernel_for(int mode, bool fast) {
   switch (mode) {
-    case SS_MODE_FORWARD: return fast ? solve_kernel<SS_MODE_FORWARD, true> : solve_kernel<SS_MODE_FORWARD, false>;
-    case SS_MODE_GRADIENT: return fast ? solve_kernel<SS_MODE_GRADIENT, true> : solve_kernel<SS_MODE_GRADIENT, false>;
-    case SS_MODE_SEGMENT: return fast ? solve_kernel<SS_MODE_SEGMENT, true> : solve_kernel<SS_MODE_SEGMENT, false>;
-    default: return fast ? solve_kernel<SS_MODE_IMAGES, true> : solve_kernel<SS_MODE_IMAGES, false>;
+    case SS_MODE_FORWARD:
+      return fast ? solve_kernel<SS_MODE_FORWARD, true, false> : solve_kernel<SS_MODE_FORWARD, false, false>;
+    case SS_MODE_GRADIENT:
+      return fast ? solve_kernel<SS_MODE_GRADIENT, true, false> : solve_kernel<SS_MODE_GRADIENT, false, false>;
+    case SS_MODE_SEGMENT:
+      return fast ? solve_kernel<SS_MODE_SEGMENT, true, false> : solve_kernel<SS_MODE_SEGMENT, false, false>;
+    default: return fast ? solve_kernel<SS_MODE_IMAGES, true, false> : solve_kernel<SS_MODE_IMAGES, false, false>;
+  }
+}
+
+// Uneven batches: one generic instantiation per mode, geometry per solve.
+SolveFn batch_kernel_for(int mode) {
+  switch (mode) {
+    case SS_MODE_FORWARD: return solve_kernel<SS_MODE_FORWARD, false, true>;
+    case SS_MODE_GRADIENT: return solve_kernel<SS_MODE_GRADIENT, false, true>;
+    default: return solve_kernel<SS_MODE_IMAGES, false, true>;
   }
 }
 
@@ -1321,6 +1446,460 @@ int noalloc_scratch(void** out) {
     g_noalloc_address[dev] = p;
   }
   *out = g_noalloc_address[dev];
+  return SS_OK;
+}
+
+// ----------------------------------------------------------------------------
+// Uneven batches: planner (host) and runner
+// ----------------------------------------------------------------------------
+// A plan is one contiguous blob, identical in host and device memory:
+// BatchPlanHeader, then BatchItemDev[n_items], then int order[n_solves]
+// (per class, solves longest-first).  The header carries the launch shapes.
+constexpr uint64_t kPlanMagic = 0x3130504853535342ull;   // "BSSSHP01"
+
+struct BatchClassHost {
+  int C, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter;
+  int max_clusters, idle_sms;   // co-resident clusters alone on the GPU, and the SMs they leave idle
+  size_t hist_slot, trace_slot, gpad_slot, grad_slot;   // floats per slot
+  size_t ws_off;                                        // bytes: this class's scratch in the workspace
+  double cell_steps;
+};
+
+struct BatchPlanHeader {
+  uint64_t magic;
+  int32_t mode, n_items, n_solves, n_classes, max_nt, concurrent;
+  int64_t total_bytes, ws_bytes, items_off, order_off;
+  double dtdx2, amp_ref, dx, dt;
+  BatchClassHost cls[kMaxCluster];
+};
+
+// Shared memory of a batch launch: the fixed part (barriers, wavelet,
+// reduction words, residual rows, receiver ring) and one solve's part
+// (two fields, the history slabs, the zero tile).
+size_t batch_fixed_smem(int nt_max, int nxs) {
+  return (16 + static_cast<size_t>((nt_max + 31) & ~31) + 32 + static_cast<size_t>(kStages + kTraceRing) * nxs) *
+         sizeof(float);
+}
+size_t batch_solve_smem(int bh, int ncg, bool adj) {
+  constexpr int H = kRowsPerThread;
+  const size_t rs = 4 * static_cast<size_t>(ncg) + 8, sw = 4 * static_cast<size_t>(ncg);
+  return (2 * (bh + 4) * rs + (adj ? kStages * bh * sw : 0) + (H + 4) * rs + H * sw) * sizeof(float);
+}
+
+int item_ncg(const ss_batch_item& it) { return (it.nx + 2 * it.pad - 4 + 3) / 4; }
+
+struct ItemShape {
+  int nseg, bh, nact;
+};
+// Band shape of one item at cluster size C; nact > kMaxThreads means it does not fit.
+ItemShape item_shape(const ss_batch_item& it, int C) {
+  constexpr int H = kRowsPerThread;
+  const int nrows = it.nz + 2 * it.pad - 4;
+  const int ncg = item_ncg(it);
+  ItemShape s;
+  s.nseg = (nrows + C * H - 1) / (C * H);
+  s.bh = s.nseg * H;
+  s.nact = ncg * s.nseg;
+  return s;
+}
+bool item_fits(const ss_batch_item& it, int C, bool adj) {
+  const ItemShape s = item_shape(it, C);
+  const int ncg = item_ncg(it);
+  return s.nact <= kMaxThreads &&
+         batch_fixed_smem(it.nt, (it.nx + 3) & ~3) + batch_solve_smem(s.bh, ncg, adj) <= kMaxSmem;
+}
+
+struct DeviceStreams {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_stream_mutex;
+DeviceStreams g_streams[64];
+
+// The library's second stream and its fork/join events on the current device,
+// created once (plan time, so that runs under stream capture create nothing).
+int device_streams(DeviceStreams** out) {
+  int dev = 0;
+  SS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SS_ERR_UNSUPPORTED, "device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_stream_mutex);
+  DeviceStreams& d = g_streams[dev];
+  if (!d.side) {
+    SS_CUDA(cudaStreamCreateWithFlags(&d.side, cudaStreamNonBlocking));
+    SS_CUDA(cudaEventCreateWithFlags(&d.fork, cudaEventDisableTiming));
+    SS_CUDA(cudaEventCreateWithFlags(&d.join, cudaEventDisableTiming));
+  }
+  *out = &d;
+  return SS_OK;
+}
+
+// Dynamic shared memory limit of a batch instantiation on the current
+// device, raised (never lowered) as plans need more; a run whose plan set it
+// already makes no attribute call.
+std::mutex g_attr_mutex;
+int g_batch_smem[64][3] = {};
+int ensure_batch_smem(int mode, int bytes) {
+  int dev = 0;
+  SS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SS_ERR_UNSUPPORTED, "device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  int& cur = g_batch_smem[dev][mode];
+  if (bytes <= cur) return SS_OK;
+  const void* fn = reinterpret_cast<const void*>(batch_kernel_for(mode));
+  SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cur = bytes;
+  return SS_OK;
+}
+
+int check_item(const ss_batch_item& it, int i) {
+  const std::string at = "item " + std::to_string(i) + ": ";
+  if (it.nz < 1 || it.nx < 1 || it.nt < 1) return fail(SS_ERR_INVALID, at + "nz, nx and nt must be positive");
+  if (it.pad < 2) return fail(SS_ERR_INVALID, at + "pad must be >= 2");
+  if (it.n_shots < 1 || it.n_shots > SS_MAX_SHOTS) return fail(SS_ERR_INVALID, at + "n_shots must lie in 1..16");
+  if (it.src_row < 0 || it.src_row >= it.nz) return fail(SS_ERR_INVALID, at + "src_row outside the model");
+  for (int s = 0; s < it.n_shots; ++s)
+    if (it.shot_cols[s] < 0 || it.shot_cols[s] >= it.nx) return fail(SS_ERR_INVALID, at + "shot column outside the model");
+  if (it.vel_offset < 0 || it.obs_offset < 0 || it.out_offset < 0) return fail(SS_ERR_INVALID, at + "negative offset");
+  return SS_OK;
+}
+
+int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int n_items, const int* cluster_by_class,
+               int concurrent, void* plan, size_t* plan_bytes, size_t* ws_bytes) {
+  if (!phys || !items || n_items < 1 || !plan_bytes || !ws_bytes) return fail(SS_ERR_INVALID, "bad arguments");
+  if (mode != SS_MODE_FORWARD && mode != SS_MODE_GRADIENT && mode != SS_MODE_IMAGES)
+    return fail(SS_ERR_INVALID, "mode must be forward, gradient or images");
+  if (!(phys->dx > 0.0) || !(phys->dt > 0.0) || !(phys->r_coef > 0.0) || !(phys->r_coef < 1.0) ||
+      !(phys->vmax_damping > 0.0) || !(phys->amp_ref > 0.0))
+    return fail(SS_ERR_INVALID, "dx, dt, vmax_damping and amp_ref must be positive and 0 < r_coef < 1");
+  const bool adj = mode != SS_MODE_FORWARD;
+  // ---- size class of every item: its smallest fitting cluster ------------
+  std::vector<int> cl(n_items), min_c(n_items);
+  long long n_solves = 0;
+  int max_nt = 0;
+  for (int i = 0; i < n_items; ++i) {
+    const int rc = check_item(items[i], i);
+    if (rc) return rc;
+    int C = 1;
+    while (C <= kMaxCluster && !item_fits(items[i], C, adj)) ++C;
+    if (C > kMaxCluster) return fail(SS_ERR_UNSUPPORTED, "item " + std::to_string(i) + ": no cluster plan fits this grid");
+    min_c[i] = C;
+    int use = C;
+    if (cluster_by_class && cluster_by_class[C] > 0) use = std::min(kMaxCluster, std::max(C, cluster_by_class[C]));
+    cl[i] = use;
+    n_solves += items[i].n_shots;
+    max_nt = std::max(max_nt, items[i].nt);
+  }
+  if (n_solves > (1LL << 27) || n_items > (1 << 27)) return fail(SS_ERR_INVALID, "too many items");
+  // ---- classes by cluster size; a class whose combined shared memory does
+  // not fit moves its largest items one cluster size up ---------------------
+  BatchPlanHeader h{};
+  std::vector<std::vector<int>> members(kMaxCluster + 1);
+  for (int i = 0; i < n_items; ++i) members[cl[i]].push_back(i);
+  for (int C = 1; C <= kMaxCluster; ++C) {
+    for (;;) {
+      auto& m = members[C];
+      if (m.empty()) break;
+      int nt_max = 0, nxs = 0;
+      size_t solve_part = 0;
+      for (int i : m) {
+        nt_max = std::max(nt_max, items[i].nt);
+        nxs = std::max(nxs, (items[i].nx + 3) & ~3);
+        const ItemShape s = item_shape(items[i], C);
+        solve_part = std::max(solve_part, batch_solve_smem(s.bh, item_ncg(items[i]), adj));
+      }
+      if (batch_fixed_smem(nt_max, nxs) + solve_part <= kMaxSmem) break;
+      if (C == kMaxCluster) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits the batch's shared memory");
+      std::vector<int> keep;
+      for (int i : m) {
+        const ItemShape s = item_shape(items[i], C);
+        if (batch_solve_smem(s.bh, item_ncg(items[i]), adj) == solve_part)
+          members[C + 1].push_back(i);
+        else
+          keep.push_back(i);
+      }
+      if (keep.size() == m.size()) return fail(SS_ERR_UNSUPPORTED, "batch planner made no progress");
+      m.swap(keep);
+    }
+  }
+  // ---- launch shape, solve order and scratch of every class -------------
+  struct Cls {
+    int C;
+    std::vector<int> items;
+    double work;
+  };
+  std::vector<Cls> cls;
+  for (int C = 1; C <= kMaxCluster; ++C)
+    if (!members[C].empty()) {
+      double work = 0;
+      for (int i : members[C]) work += static_cast<double>(items[i].nt) * items[i].n_shots * C;
+      cls.push_back({C, members[C], work});
+    }
+  // Heaviest class first: it starts on the whole GPU; lighter ones fill tails.
+  std::stable_sort(cls.begin(), cls.end(), [](const Cls& a, const Cls& b) { return a.work > b.work; });
+  h.magic = kPlanMagic;
+  h.mode = mode;
+  h.n_items = n_items;
+  h.n_solves = static_cast<int32_t>(n_solves);
+  h.n_classes = static_cast<int32_t>(cls.size());
+  h.max_nt = max_nt;
+  h.concurrent = std::min(std::max(concurrent, 0), 2);
+  const double dtdx = phys->dt / phys->dx;
+  h.dtdx2 = dtdx * dtdx;
+  h.amp_ref = phys->amp_ref;
+  h.dx = phys->dx;
+  h.dt = phys->dt;
+  h.items_off = static_cast<int64_t>(align_up(sizeof(BatchPlanHeader)));
+  h.order_off = static_cast<int64_t>(align_up(h.items_off + sizeof(BatchItemDev) * static_cast<size_t>(n_items)));
+  h.total_bytes = static_cast<int64_t>(align_up(h.order_off + sizeof(int) * static_cast<size_t>(n_solves)));
+
+  const SolveFn fn_ptr = batch_kernel_for(mode);
+  const void* fn = reinterpret_cast<const void*>(fn_ptr);
+  std::vector<int> order;
+  order.reserve(n_solves);
+  size_t region[2] = {0, 0};
+  for (size_t c = 0; c < cls.size(); ++c) {
+    BatchClassHost& k = h.cls[c];
+    const int C = cls[c].C;
+    k.C = C;
+    k.min_C = kMaxCluster;
+    k.counter = static_cast<int>(c);
+    int max_nact = 0;
+    size_t solve_part = 0;
+    k.nt_max = 0;
+    k.nxs = 0;
+    k.bh_max = 0;
+    k.cell_steps = 0;
+    for (int i : cls[c].items) {
+      const ss_batch_item& it = items[i];
+      const ItemShape s = item_shape(it, C);
+      const int ncg = item_ncg(it);
+      k.min_C = std::min(k.min_C, min_c[i]);
+      max_nact = std::max(max_nact, s.nact);
+      solve_part = std::max(solve_part, batch_solve_smem(s.bh, ncg, adj));
+      k.nt_max = std::max(k.nt_max, it.nt);
+      k.nxs = std::max(k.nxs, (it.nx + 3) & ~3);
+      k.bh_max = std::max(k.bh_max, s.bh);
+      const size_t nzp = it.nz + 2 * it.pad, nxp = it.nx + 2 * it.pad;
+      k.hist_slot = std::max(k.hist_slot, static_cast<size_t>(it.nt) * C * s.bh * 4 * ncg);
+      k.gpad_slot = std::max(k.gpad_slot, nzp * nxp);
+      k.grad_slot = std::max(k.grad_slot, static_cast<size_t>(it.nz) * it.nx);
+      k.cell_steps += static_cast<double>(nzp) * nxp * it.nt * it.n_shots;
+    }
+    k.trace_slot = static_cast<size_t>(k.nt_max) * k.nxs;
+    k.threads = ((max_nact + 31) / 32) * 32;
+    k.smem = static_cast<int>(batch_fixed_smem(k.nt_max, k.nxs) + solve_part);
+    // solves longest-first
+    const int begin = static_cast<int>(order.size());
+    for (int i : cls[c].items)
+      for (int s = 0; s < items[i].n_shots; ++s) order.push_back(i << 4 | s);
+    std::stable_sort(order.begin() + begin, order.end(),
+                     [&](int a, int b) { return items[a >> 4].nt > items[b >> 4].nt; });
+    k.order_begin = begin;
+    k.n_solves = static_cast<int>(order.size()) - begin;
+    // persistent clusters: as many as fit on the device at once
+    int rc = ensure_batch_smem(mode, k.smem);
+    if (rc) return rc;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C, 1, 1);
+    cfg.blockDim = dim3(k.threads, 1, 1);
+    cfg.dynamicSmemBytes = k.smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg);
+    if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaOccupancyMaxActiveClusters: ") + cudaGetErrorString(e));
+    if (nclusters < 1) return fail(SS_ERR_UNSUPPORTED, "no cluster of a batch class fits on the device");
+    k.slots = std::max(1, std::min(nclusters, k.n_solves));
+    k.max_clusters = nclusters;
+    int per_sm = 1, n_sm = 0, dev = 0;
+    SS_CUDA(cudaGetDevice(&dev));
+    SS_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    SS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, k.threads, k.smem));
+    k.idle_sms = n_sm - (nclusters * C + std::max(per_sm, 1) - 1) / std::max(per_sm, 1);
+  }
+  // ---- streams and launch order -------------------------------------------
+  // 0: one stream, heaviest class first.  1: heaviest first, alternating
+  // between two streams, so that a class's tail overlaps the next class.
+  // 2: classes whose clusters leave many SMs idle (large clusters pack GPCs
+  // badly) go first on stream 0, largest cluster first; the rest, on
+  // stream 1, fill the SMs they leave.
+  const int n_cls = static_cast<int>(cls.size());
+  std::vector<BatchClassHost> sorted(h.cls, h.cls + n_cls);
+  if (h.concurrent == 2) {
+    int n_sm = 0, dev = 0;
+    SS_CUDA(cudaGetDevice(&dev));
+    SS_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    std::vector<BatchClassHost> big, rest;
+    for (const auto& k : sorted) (k.idle_sms * 10 >= n_sm ? big : rest).push_back(k);
+    auto by_c = [](const BatchClassHost& a, const BatchClassHost& b) { return a.C > b.C; };
+    std::stable_sort(big.begin(), big.end(), by_c);
+    std::stable_sort(rest.begin(), rest.end(), by_c);
+    if (big.empty() || rest.empty()) {
+      h.concurrent = 1;
+    } else {
+      for (auto& k : big) k.stream = 0;
+      for (auto& k : rest) k.stream = 1;
+      sorted = big;
+      sorted.insert(sorted.end(), rest.begin(), rest.end());
+    }
+  }
+  if (h.concurrent != 2)
+    for (int c = 0; c < n_cls; ++c) sorted[c].stream = h.concurrent ? (c & 1) : 0;
+  for (int c = 0; c < n_cls; ++c) {
+    BatchClassHost& k = sorted[c];
+    k.counter = c;
+    size_t bytes = 0;
+    if (adj)
+      bytes = align_up(k.slots * k.hist_slot * sizeof(float)) + align_up(k.slots * k.trace_slot * sizeof(float)) +
+              align_up(k.slots * k.gpad_slot * sizeof(float)) + align_up(k.slots * k.grad_slot * sizeof(float));
+    region[k.stream] = std::max(region[k.stream], bytes);
+    h.cls[c] = k;
+  }
+  // workspace: status word and class counters, then one scratch region per stream
+  for (int c = 0; c < n_cls; ++c) h.cls[c].ws_off = 256 + (h.cls[c].stream ? region[0] : 0);
+  h.ws_bytes = static_cast<int64_t>(256 + region[0] + region[1]);
+  *plan_bytes = static_cast<size_t>(h.total_bytes);
+  *ws_bytes = static_cast<size_t>(h.ws_bytes);
+  DeviceStreams* ds = nullptr;
+  int rc = device_streams(&ds);
+  if (rc) return rc;
+  if (!plan) return SS_OK;
+  unsigned char* out = static_cast<unsigned char*>(plan);
+  std::memset(out, 0, static_cast<size_t>(h.total_bytes));
+  std::memcpy(out, &h, sizeof(h));
+  BatchItemDev* dv = reinterpret_cast<BatchItemDev*>(out + h.items_off);
+  for (int i = 0; i < n_items; ++i) {
+    const ss_batch_item& it = items[i];
+    BatchItemDev d{};
+    d.nz = it.nz;
+    d.nx = it.nx;
+    d.nt = it.nt;
+    d.pad = it.pad;
+    d.nzp = it.nz + 2 * it.pad;
+    d.nxp = it.nx + 2 * it.pad;
+    d.src_row = it.src_row;
+    d.n_shots = it.n_shots;
+    d.ncg = item_ncg(it);
+    for (int q = 0; q < SS_MAX_SHOTS; ++q) d.shot_cols[q] = q < it.n_shots ? it.shot_cols[q] : 0;
+    d.vel_off = it.vel_offset;
+    d.obs_off = it.obs_offset;
+    d.out_off = it.out_offset;
+    d.damp_k = 3.0 * phys->vmax_damping / (2.0 * it.pad * phys->dx) * std::log(1.0 / phys->r_coef) * phys->dt / 2.0;
+    d.vmute = it.v_mute;
+    dv[i] = d;
+  }
+  for (size_t c = 0; c < cls.size(); ++c)   // band shape at the class's cluster size
+    for (int i : cls[c].items) {
+      const ItemShape s = item_shape(items[i], cls[c].C);
+      dv[i].nseg = s.nseg;
+      dv[i].bh = s.bh;
+      dv[i].nact = s.nact;
+    }
+  std::memcpy(out + h.order_off, order.data(), sizeof(int) * order.size());
+  return SS_OK;
+}
+
+int batch_run(const void* plan, const void* plan_dev, const float* vel, const float* wavelet, const float* obs,
+              float t_mute, float eps, int laplacian, float* gathers, float* img, float* illum, float* grad, void* ws,
+              size_t ws_bytes, void* stream) {
+  if (!plan || !plan_dev) return fail(SS_ERR_INVALID, "plan and its device copy are required");
+  BatchPlanHeader h;
+  std::memcpy(&h, plan, sizeof(h));
+  if (h.magic != kPlanMagic) return fail(SS_ERR_INVALID, "not a batch plan");
+  const int mode = h.mode;
+  if (!vel || !wavelet) return fail(SS_ERR_INVALID, "vel and wavelet are required");
+  if (mode == SS_MODE_FORWARD && !gathers) return fail(SS_ERR_INVALID, "gathers output is required");
+  if (mode != SS_MODE_FORWARD && (!obs || !illum)) return fail(SS_ERR_INVALID, "obs and illum are required");
+  if (mode == SS_MODE_GRADIENT && !grad) return fail(SS_ERR_INVALID, "grad output is required");
+  if (mode == SS_MODE_IMAGES && !img) return fail(SS_ERR_INVALID, "img output is required");
+  if (mode == SS_MODE_IMAGES && !(eps > 0.f)) return fail(SS_ERR_INVALID, "illumination regularization eps must be positive");
+  if (!ws || ws_bytes < static_cast<size_t>(h.ws_bytes)) return fail(SS_ERR_WORKSPACE, "workspace missing or too small");
+  DeviceStreams* ds = nullptr;
+  int rc = device_streams(&ds);
+  if (rc) return rc;
+  unsigned char* w = static_cast<unsigned char*>(ws);
+  const unsigned char* pd = static_cast<const unsigned char*>(plan_dev);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SS_CUDA(cudaMemsetAsync(w, 0, 256, st));
+  const SolveFn fn_ptr = batch_kernel_for(mode);
+  int max_smem = 0;
+  bool two = false;
+  for (int c = 0; c < h.n_classes; ++c) {
+    max_smem = std::max(max_smem, h.cls[c].smem);
+    two = two || h.cls[c].stream == 1;
+  }
+  rc = ensure_batch_smem(mode, max_smem);
+  if (rc) return rc;
+  if (two) {
+    SS_CUDA(cudaEventRecord(ds->fork, st));
+    SS_CUDA(cudaStreamWaitEvent(ds->side, ds->fork, 0));
+  }
+  for (int c = 0; c < h.n_classes; ++c) {
+    const BatchClassHost& k = h.cls[c];
+    KParams p{};
+    p.C = k.C;
+    p.nt = k.nt_max;
+    p.nxs = k.nxs;
+    p.bh = k.bh_max;
+    p.n_solves = k.n_solves;
+    p.items = reinterpret_cast<const BatchItemDev*>(pd + h.items_off);
+    p.order = reinterpret_cast<const int*>(pd + h.order_off) + k.order_begin;
+    p.counter = reinterpret_cast<int*>(w + 64) + k.counter;
+    p.dtdx2 = h.dtdx2;
+    p.amp_ref = h.amp_ref;
+    p.dx = static_cast<float>(h.dx);
+    p.dt = static_cast<float>(h.dt);
+    p.vel = vel;
+    p.wav = wavelet;
+    p.obs = obs;
+    p.t_mute = t_mute;
+    p.gathers = gathers;
+    p.illum = illum;
+    p.img = img;
+    p.eps = eps;
+    p.laplacian = laplacian;
+    p.err = reinterpret_cast<int*>(w);
+    p.ckpt_interval = 1;
+    p.hist_slot = k.hist_slot;
+    p.trace_slot = k.trace_slot;
+    p.gpad_slot = k.gpad_slot;
+    p.grad_slot = k.grad_slot;
+    if (mode != SS_MODE_FORWARD) {
+      unsigned char* r = w + k.ws_off;
+      p.hist = reinterpret_cast<float*>(r);
+      r += align_up(k.slots * k.hist_slot * sizeof(float));
+      p.trace = reinterpret_cast<float*>(r);
+      r += align_up(k.slots * k.trace_slot * sizeof(float));
+      p.gpad = reinterpret_cast<float*>(r);
+      r += align_up(k.slots * k.gpad_slot * sizeof(float));
+      p.grad_per_slot = grad == nullptr;
+      p.grad = grad ? grad : reinterpret_cast<float*>(r);
+    }
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = k.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(k.C * k.slots, 1, 1);
+    cfg.blockDim = dim3(k.threads, 1, 1);
+    cfg.dynamicSmemBytes = k.smem;
+    cfg.stream = k.stream ? ds->side : st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn_ptr, p);
+    if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaLaunchKernelEx: ") + cudaGetErrorString(e));
+  }
+  if (two) {
+    SS_CUDA(cudaEventRecord(ds->join, ds->side));
+    SS_CUDA(cudaStreamWaitEvent(st, ds->join, 0));
+  }
   return SS_OK;
 }
 
@@ -1617,6 +2196,54 @@ int32_t ss_c2_field(const ss_geometry* geom, int32_t n_models, const float* vel,
                                                                            geom->pad, dtdx * dtdx);
   SS_CUDA(cudaGetLastError());
   return SS_OK;
+}
+
+int32_t ss_batch_plan(const ss_physics* phys, int32_t mode, const ss_batch_item* items, int32_t n_items,
+                      const int32_t* cluster_by_class, int32_t concurrent, void* plan, size_t* plan_bytes,
+                      size_t* workspace_bytes) {
+  g_last_error.clear();
+  return batch_plan(phys, mode, items, n_items, cluster_by_class, concurrent, plan, plan_bytes, workspace_bytes);
+}
+
+int32_t ss_batch_min_cluster(const ss_batch_item* item, int32_t mode) {
+  g_last_error.clear();
+  if (!item) return fail(SS_ERR_INVALID, "item is NULL");
+  int rc = check_item(*item, 0);
+  if (rc) return rc;
+  for (int C = 1; C <= kMaxCluster; ++C)
+    if (item_fits(*item, C, mode != SS_MODE_FORWARD)) return C;
+  return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits this grid");
+}
+
+int32_t ss_batch_classes(const void* plan, ss_batch_class_info* out, int32_t max_classes, int32_t* n_classes) {
+  g_last_error.clear();
+  if (!plan || !n_classes || (max_classes > 0 && !out)) return fail(SS_ERR_INVALID, "bad arguments");
+  BatchPlanHeader h;
+  std::memcpy(&h, plan, sizeof(h));
+  if (h.magic != kPlanMagic) return fail(SS_ERR_INVALID, "not a batch plan");
+  *n_classes = h.n_classes;
+  for (int c = 0; c < std::min<int>(h.n_classes, max_classes); ++c) {
+    const BatchClassHost& k = h.cls[c];
+    ss_batch_class_info& o = out[c];
+    o.min_cluster = k.min_C;
+    o.cluster = k.C;
+    o.n_solves = k.n_solves;
+    o.threads = k.threads;
+    o.smem_bytes = k.smem;
+    o.slots = k.slots;
+    o.stream = k.stream;
+    o.reserved = 0;
+    o.cell_steps = k.cell_steps;
+  }
+  return SS_OK;
+}
+
+int32_t ss_batch_run(const void* plan, const void* plan_device, const float* vel, const float* wavelet,
+                     const float* obs, float t_mute, float eps, int32_t laplacian, float* gathers, float* img,
+                     float* illum, float* grad, void* workspace, size_t workspace_bytes, void* stream) {
+  g_last_error.clear();
+  return batch_run(plan, plan_device, vel, wavelet, obs, t_mute, eps, laplacian, gathers, img, illum, grad, workspace,
+                   workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -103,3 +103,44 @@ def population(n=500, nz=70, nx=70, tag=1):
 def small_model(seed=0, nz=70, nx=70):
     """The single curved 3-5-layer model of the small plain-method case."""
     return model('curved', seed, nz, nx)
+
+
+RHOS = (0.6, 1.0, 1.4)   # slow / medium / fast background factors of the depth trend
+
+
+def uneven_workload(n_solves=2000, seed=2, nz_range=(70, 200), nx_range=(70, 300), nt_range=(1000, 3000),
+                    shots_range=(1, 9), bgs_range=(1, 3)):
+    """Seeded models of uneven size for batched RTM, until `n_solves` (model, background, shot) solves.
+
+    Per model: nz, nx, nt, shot count and background count drawn uniformly from the
+    ranges (inclusive), family cycling through FAMILIES, shots at
+    round(linspace(0, nx - 1, n)), backgrounds clip(v_s + rho * trend) for the
+    first `n_bg` of a seeded permutation of RHOS, with v_s the model's top-row
+    mean and trend its own lateral-mean depth profile minus v_s.  The last model's
+    shots are cut so that the total is exactly `n_solves`.
+    Returns a list of dicts: truth [nz, nx], backgrounds [n_bg, nz, nx], nt, shot_cols, v_s.
+    """
+    rng = np.random.default_rng([seed, 7])
+    out, total, i = [], 0, 0
+    while total < n_solves:
+        nz = int(rng.integers(nz_range[0], nz_range[1] + 1))
+        nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+        nt = int(rng.integers(nt_range[0], nt_range[1] + 1))
+        ns = int(rng.integers(shots_range[0], shots_range[1] + 1))
+        nb = int(rng.integers(bgs_range[0], bgs_range[1] + 1))
+        rhos = [RHOS[j] for j in rng.permutation(len(RHOS))[:nb]]
+        left = n_solves - total
+        if ns * nb > left:                       # trim the last model
+            nb = min(nb, left)
+            ns = max(1, left // nb)
+            nb = left // ns
+            rhos = rhos[:nb]
+        truth = model(FAMILIES[i % len(FAMILIES)], [seed, i], nz, nx)
+        v_s = float(truth[0].astype(np.float64).mean())
+        trend = truth.astype(np.float64).mean(1) - v_s
+        bgs = np.stack([np.tile(np.clip(v_s + r * trend, VMIN, VMAX)[:, None], (1, nx)) for r in rhos])
+        cols = [int(c) for c in np.round(np.linspace(0, nx - 1, ns))]
+        out.append(dict(truth=truth, backgrounds=bgs.astype(np.float32), nt=nt, shot_cols=cols, v_s=v_s))
+        total += ns * nb
+        i += 1
+    return out

@@ -100,3 +100,50 @@ def test_memory_model_is_bounded():
     full_history = 24 * 5 * 1000 * 150 * 150 * 4
     assert gpu.imaging_memory_bytes(24) < full_history         # history is shared by solves in flight
     assert gpu.imaging_memory_bytes(1) < gpu.imaging_memory_bytes(300)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors have the sizes and field offsets that a C compiler gives the header's structs."""
+    import ctypes
+    import shutil
+    import subprocess
+    from shotsweep_b200 import _lib
+    cc = shutil.which('gcc') or shutil.which('cc')
+    if cc is None:
+        pytest.skip('no C compiler')
+    structs = {'ss_geometry': _lib.Geometry, 'ss_batch_item': _lib.BatchItem, 'ss_physics': _lib.Physics,
+               'ss_batch_class_info': _lib.BatchClassInfo}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "shotsweep.h"', 'int main(void) {']
+    expect = []
+    for cname, py in structs.items():
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        expect.append(ctypes.sizeof(py))
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {fname}));')
+            expect.append(getattr(py, fname).offset)
+    lines += ['  return 0;', '}']
+    src = tmp_path / 'layout.c'
+    src.write_text('\n'.join(lines))
+    exe = tmp_path / 'layout'
+    subprocess.run([cc, '-std=c99', f'-I{ROOT / "include"}', str(src), '-o', str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect
+
+
+def test_batch_size_class_and_plan_validation_without_gpu(lib):
+    """The size class of a model is host arithmetic; plans reject bad items before touching a device."""
+    import ctypes
+    from shotsweep_b200 import _lib
+    from shotsweep_b200.batch import Shape, make_items, physics
+    items, _ = make_items([Shape(70, 70, 1000, [0, 17, 34, 52, 69])])
+    assert lib.ss_batch_min_cluster(items, _lib.MODE_IMAGES) == 3      # 150 x 150 padded: three 50-row bands
+    items, _ = make_items([Shape(100, 300, 90, [0, 150, 299])])
+    assert lib.ss_batch_min_cluster(items, _lib.MODE_IMAGES) == 9      # 95 column groups: 20-row bands
+    items, _ = make_items([Shape(20, 20, 50, [3], pad=5, src_row=20)])
+    assert lib.ss_batch_min_cluster(items, _lib.MODE_IMAGES) == _lib.ERR_INVALID
+    pb, wb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    rc = lib.ss_batch_plan(ctypes.byref(physics()), _lib.MODE_IMAGES, items, 1, None, 1, None, ctypes.byref(pb),
+                           ctypes.byref(wb))
+    assert rc == _lib.ERR_INVALID and b'src_row' in lib.ss_last_error()
+    rc = lib.ss_batch_plan(ctypes.byref(physics()), 7, items, 1, None, 1, None, ctypes.byref(pb), ctypes.byref(wb))
+    assert rc == _lib.ERR_INVALID and b'mode' in lib.ss_last_error()
