@@ -66,7 +66,7 @@ def parse():
     ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
     ap.add_argument('--models', type=int, default=N_MODELS, help='velocity models per GPU')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--workload', choices=('openfwi', 'uneven'), default='openfwi')
+    ap.add_argument('--workload', choices=('openfwi', 'uneven', 'process'), default='openfwi')
     ap.add_argument('--solves', type=int, default=2000, help='uneven workload: solves per GPU')
     ap.add_argument('--schedule', type=int, default=-1, choices=(-1, 0, 1, 2),
                     help='uneven workload: stream schedule (-1: autotuned)')
@@ -437,6 +437,87 @@ def run_uneven(args):
     return 0
 
 
+def run_process(args):
+    """2_process's per-batch work for the 500-model population: picks, backgrounds, images, float16 cache."""
+    import torch
+    from oracle import postprocess as PP
+    from shotsweep_b200 import background as BG
+    from shotsweep_b200 import dist as D
+    from shotsweep_b200 import engine, gpu, process
+    rank, world, local = D.init('nccl' if args.gpus > 1 else 'gloo', timeout_s=300)
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    per = args.models
+    a, b = D.shard(per * world, rank, world)
+    # the first `per` models of a seeded pool whose first arrivals the picker accepts (2_process refuses a
+    # batch with any rejected model)
+    pool = population_slice(2 * a, 2 * b, 2 * per * world)
+    trend = depth_trend(population_slice(0, N_MODELS, N_MODELS))
+    sim = gpu.Sim(device=dev)
+    eng = sim.engine
+    pool_g = eng.forward(torch.tensor(pool, dtype=torch.float32, device=dev), engine.scaled_wavelet(gpu.RICKER, dev))
+    ok = np.flatnonzero([e.status == 0 for e in BG.surface_estimates(pool_g)])[:per]
+    if len(ok) < per:
+        raise SystemExit(f'only {len(ok)} of {len(pool)} pool models have usable first arrivals')
+    gathers = pool_g[torch.tensor(ok, device=dev)].contiguous()
+    del pool_g
+    v1 = np.array([e['velocity'] for e in BG.estimate_surface_velocity_batch(gathers)])
+    bgs = BG.backgrounds(v1, trend, device=dev).reshape(per * 3, 70, 70)
+    img, _ = eng.images(bgs, sim._wavelet(), gathers.repeat_interleave(3, dim=0),
+                        torch.tensor(np.repeat(v1, 3), dtype=torch.float32, device=dev))
+    times = {'surface': [], 'cache': [], 'batch': []}
+
+    def timed(name, fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times[name].append(e0.elapsed_time(e1))
+        return r
+
+    for step in range(args.warmup + args.steps):
+        est = timed('surface', lambda: BG.surface_estimates(gathers))
+        cache = timed('cache', lambda: process.image_cache(img.view(per, 3, 5, 70, 70)))
+        out = timed('batch', lambda: process.process_batch(sim, gathers, trend))
+        if step < args.warmup:
+            for k in times:
+                times[k].clear()
+    eng.status()
+    ms = {k: D.reduce(statistics.mean(v), 'max', dev if world > 1 else None) for k, v in times.items()}
+    value = world * per / (ms['batch'] * 1e-3)
+    # CPU: the NumPy restatement of the picks and the cache on a sample of 20 models, one thread each step
+    g_host = gathers[:20].cpu().numpy().astype(np.float64)
+    t0 = time.perf_counter()
+    for k in range(20):
+        try:
+            PP.estimate_surface_velocity(g_host[k])
+        except ValueError:
+            pass
+    cpu_surface = 20 / (time.perf_counter() - t0)
+    im_host = out['images'][:20].float().cpu().numpy()
+    t0 = time.perf_counter()
+    PP.image_cache(im_host)
+    cpu_cache = 20 / (time.perf_counter() - t0)
+    if rank == 0:
+        print(json.dumps({
+            'metric': '2_process models/s (surface picks + 3 backgrounds + 15 RTM images + float16 cache per model)',
+            'value': value, 'unit': 'models/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': ms['batch'], 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32', 'data': 'synthetic: the 500-model OpenFWI-shaped population, gathers simulated',
+            'config': {'workload': f'{per} models per GPU per step (the first with usable first arrivals of a '
+                                   f'{len(pool)}-model seeded pool)', 'models_per_gpu': per},
+            'kernels': {'surface_velocity_models_per_s': per / (ms['surface'] * 1e-3),
+                        'image_cache_models_per_s': per / (ms['cache'] * 1e-3)},
+            'cpu_baseline': {'surface_velocity_models_per_s': cpu_surface, 'image_cache_models_per_s': cpu_cache,
+                             'unit': 'models/s', 'cores': 1, 'kind': 'port',
+                             'sample': '20 models, NumPy restatement of background.py:19-83 and 2_process.py:206-210'},
+            'gpu_launches': None,
+        }), flush=True)
+    D.finish()
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 0 or args.steps < 1:
@@ -445,6 +526,8 @@ def main():
         return run_reference(args)
     if args.workload == 'uneven':
         return run_uneven(args)
+    if args.workload == 'process':
+        return run_process(args)
     return run_ours(args)
 
 

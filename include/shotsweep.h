@@ -273,6 +273,65 @@ int32_t ss_batch_run(const void* plan, const void* plan_device, const float* vel
                      const float* obs, float t_mute, float eps, int32_t laplacian, float* gathers, float* img,
                      float* illum, float* grad, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- After the images: 2_process's cache epilogue, surface velocity and
+ * training inputs (no FFI in the reference: these replace NumPy code that
+ * 2_process.py and 3_train.py run on the host per model) ---- */
+
+/* First-arrival surface velocity of one model's gathers
+ * (background.py:19-83, estimate_surface_velocity): onsets at the first sample
+ * whose |amplitude| exceeds frac x the trace's peak, line fits of the median
+ * onset time per offset at 10-60 m, curvature, shot-to-shot spread and the
+ * far-offset (120-250 m) refraction check.  status: SS_SURF_OK or the
+ * reference's reason for raising ValueError. */
+typedef enum ss_surface_status {
+    SS_SURF_OK = 0,
+    SS_SURF_NO_ONSETS = 1,    /* no nonzero onset traces                      */
+    SS_SURF_FEW_NEAR = 2,     /* not exactly six distinct 10-60 m offsets      */
+    SS_SURF_SLOPE = 3,        /* short-offset velocity outside 1400-4600 m/s   */
+    SS_SURF_FEW_SHOTS = 4,    /* fewer than three shots with 4 near offsets    */
+    SS_SURF_UNRELIABLE = 5,   /* RMSE > 2 ms, curvature or spread > 0.15       */
+    SS_SURF_NONFINITE = 6     /* non-finite samples                           */
+} ss_surface_status;
+
+typedef struct ss_surface_estimate {
+    double velocity;                 /* clip(1 / slope, 1500, 4500) m/s        */
+    double confidence;
+    double fit_rmse_ms;
+    double short_offset_curvature;
+    double shot_slope_spread;
+    double far_offset_velocity;      /* NaN when the far slope is not positive */
+    int32_t possible_refraction;
+    int32_t status;                  /* ss_surface_status                      */
+} ss_surface_estimate;
+
+/* gathers [n_models][n_shots][nt][nx] f32 (device); src_x: HOST array of the
+ * n_shots source positions in metres; out [n_models] (device). */
+int32_t ss_surface_velocity(const float* gathers, int32_t n_models, int32_t n_shots, int32_t nt, int32_t nx,
+                            const double* src_x, double dx, double dt, double frac, ss_surface_estimate* out,
+                            void* stream);
+/* Laterally constant backgrounds clip(v_surface[m] + rhos[k] trend[z], 1500, 4500)
+ * (background.py:97-99) in float64, stored as f32 [n_models][n_rhos][nz][nx]. */
+int32_t ss_backgrounds(const double* v_surface, const double* trend, const double* rhos, int32_t n_models,
+                       int32_t n_rhos, int32_t nz, int32_t nx, float* out, void* stream);
+/* The image cache of 2_process.py:206-210: per model, rows [0, zero_rows) of
+ * every image zeroed, scale = the q-th percentile of |img| over the model's
+ * n_images x nz x nx values (NumPy's linear interpolation on float32 data),
+ * out = binary16(clip(img / scale, -clip, clip)).  img and out
+ * [n_models][n_images][nz][nx]; scale [n_models] f32; status [n_models]:
+ * SS_OK, SS_ERR_NONFINITE or SS_ERR_INVALID (scale <= 0), which 2_process
+ * turns into ValueError. */
+int32_t ss_image_cache(const float* img, int32_t n_models, int32_t n_images, int32_t nz, int32_t nx,
+                       int32_t zero_rows, double q, float clip, uint16_t* out, float* scale, int32_t* status,
+                       void* stream);
+/* Training inputs: the stored form binary16(sign(g) log1p(|g|)) (3_train.py:157),
+ * and a batch's float32 copy of it divided by the normalisation scale (3_train.py:198). */
+int32_t ss_signed_log1p_f16(const float* g, int64_t n, uint16_t* out, void* stream);
+int32_t ss_f16_scaled(const uint16_t* in, int64_t n, float scale, float* out, void* stream);
+/* Training targets (3_train.py:158,188-189): y = (vel - 3000) / 1500 over n values, and
+ * when vref is given, vref [n_models][nz][nx] = clip((v_surface[m] + trend[z] - 3000) / 1500, -1, 1). */
+int32_t ss_velocity_targets(const float* vel, int64_t n, float* y, const float* v_surface, const float* trend,
+                            int32_t n_models, int32_t nz, int32_t nx, float* vref, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

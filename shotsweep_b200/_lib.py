@@ -62,6 +62,15 @@ class BatchClassInfo(ctypes.Structure):
                 ('stream', ctypes.c_int32), ('reserved', ctypes.c_int32), ('cell_steps', ctypes.c_double)]
 
 
+class SurfaceEstimate(ctypes.Structure):
+    """Mirror of ss_surface_estimate."""
+    _fields_ = [('velocity', ctypes.c_double), ('confidence', ctypes.c_double), ('fit_rmse_ms', ctypes.c_double),
+                ('short_offset_curvature', ctypes.c_double), ('shot_slope_spread', ctypes.c_double),
+                ('far_offset_velocity', ctypes.c_double), ('possible_refraction', ctypes.c_int32),
+                ('status', ctypes.c_int32)]
+
+
+SURF_OK, SURF_NO_ONSETS, SURF_FEW_NEAR, SURF_SLOPE, SURF_FEW_SHOTS, SURF_UNRELIABLE, SURF_NONFINITE = range(7)
 MAX_CLUSTER = 16
 
 _P = ctypes.c_void_p
@@ -102,6 +111,17 @@ _SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_int32)]),
     'ss_batch_run': (ctypes.c_int32, [_P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_int32, _P, _P, _P,
                                       _P, _P, ctypes.c_size_t, _P]),
+    'ss_surface_velocity': (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, _P, _P]),
+    'ss_backgrounds': (ctypes.c_int32, [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        _P, _P]),
+    'ss_image_cache': (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_double, ctypes.c_float, _P, _P, _P, _P]),
+    'ss_signed_log1p_f16': (ctypes.c_int32, [_P, ctypes.c_int64, _P, _P]),
+    'ss_f16_scaled': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_float, _P, _P]),
+    'ss_velocity_targets': (ctypes.c_int32, [_P, ctypes.c_int64, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32, _P, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

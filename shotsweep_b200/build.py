@@ -15,8 +15,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-SOURCES = [HERE / 'csrc' / 'shotsweep.cu']
-HEADERS = [ROOT / 'include' / 'shotsweep.h']
+SOURCES = sorted((HERE / 'csrc').glob('*.cu'))
+HEADERS = [ROOT / 'include' / 'shotsweep.h', *sorted((HERE / 'csrc').glob('*.h'))]
 LIBRARY = HERE / 'libshotsweep.so'
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 

@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "../../include/shotsweep.h"
+#include "internal.h"
 
 namespace {
 
@@ -1904,6 +1905,11 @@ int batch_run(const void* plan, const void* plan_dev, const float* vel, const fl
 }
 
 }  // namespace
+
+namespace ss_internal {
+int fail(int code, const std::string& msg) { return ::fail(code, msg); }
+void clear_error() { g_last_error.clear(); }
+}  // namespace ss_internal
 
 // ============================================================================
 // C ABI

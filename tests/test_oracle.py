@@ -1,5 +1,6 @@
 """The CPU oracle against golden vectors that the reference itself produced (tests/golden)."""
 import numpy as np
+from pathlib import Path
 import pytest
 import torch
 
@@ -72,3 +73,48 @@ def test_oracle_background_helpers(plain):
     trend = O.depth_trend(synth.population(500))
     np.testing.assert_allclose(trend, plain['trend'], rtol=1e-12)
     np.testing.assert_allclose(O.backgrounds(float(plain['v_surface']), trend), plain['backgrounds'], rtol=1e-12)
+
+
+# ---- steps around the images: surface velocity, image cache, training inputs ----------------
+
+def process_case(name):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location('make_golden_process',
+                                                  Path(__file__).parent / 'golden' / 'make_golden_process.py')
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    g = golden('process_small')
+    names = [str(n) for n in g['names']]
+    base = {n: g['gathers'][i] for i, n in enumerate(mk.SIMULATED)}
+    data = {**{k: v.astype(np.float32) for k, v in base.items()}, **mk.derived(base)}
+    return names, data, g
+
+
+def test_surface_velocity_oracle_matches_reference_outputs():
+    from oracle import postprocess as PP
+    names, data, g = process_case(None)
+    keys = [str(k) for k in g['keys']]
+    for i, name in enumerate(names):
+        err = str(g['errors'][i])
+        if err:
+            with pytest.raises(ValueError) as info:
+                PP.estimate_surface_velocity(data[name].astype(np.float64))
+            assert str(info.value) == err, name
+        else:
+            est = PP.estimate_surface_velocity(data[name].astype(np.float64))
+            got = np.array([float(est[k]) for k in keys])
+            np.testing.assert_allclose(got, g['results'][i], rtol=1e-12, atol=1e-15, err_msg=name)
+
+
+def test_image_cache_oracle_is_the_reference_epilogue():
+    """The restatement applies 2_process.py:206-210 verbatim; check its properties on the reference images."""
+    from oracle import postprocess as PP
+    img = golden('plain_small')['images'][None]            # [1, 3, 5, 70, 70]
+    cache, scale = PP.image_cache(img)
+    assert cache.dtype == np.float16 and cache.shape == img.shape
+    assert np.all(cache[..., :2, :] == 0) and np.abs(cache.astype(np.float32)).max() <= 4
+    a = np.abs(img.copy())
+    a[..., :2, :] = 0
+    assert scale[0] == np.percentile(a.reshape(1, -1), 99, axis=1)[0]
+    with pytest.raises(ValueError):
+        PP.image_cache(np.zeros_like(img))
