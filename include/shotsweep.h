@@ -332,6 +332,28 @@ int32_t ss_f16_scaled(const uint16_t* in, int64_t n, float scale, float* out, vo
 int32_t ss_velocity_targets(const float* vel, int64_t n, float* y, const float* v_surface, const float* trend,
                             int32_t n_models, int32_t nz, int32_t nx, float* vref, void* stream);
 
+/* ---- Learned velocity proposal: tensor-core kernels (no counterpart in the
+ * reference's physics; its networks are PyTorch modules, 3_train.py:219-260) ---- */
+
+/* C[M][N] = A[M][K] . B[N][K]^T on the tcgen05 tensor cores: A and B BF16,
+ * row-major with K innermost (row strides lda, ldb in elements, multiples of
+ * 8, 16-byte aligned bases), F32 accumulation in tensor memory.  Epilogues:
+ *   SS_EPI_F32             C (float) = acc
+ *   SS_EPI_F32_ADD         C (float) += acc (atomic; the K loop may be split
+ *                          over `splits` CTAs, 0 = chosen to fill the GPU)
+ *   SS_EPI_BIAS_LRELU_BF16 C (BF16) = leaky_relu(acc + bias[n], slope)
+ *   SS_EPI_BIAS_F32        C (float) = acc + bias[n] (bias may be NULL)
+ * err: device int, set non-zero if a bounded wait of the pipeline ran out. */
+typedef enum ss_gemm_epilogue {
+    SS_EPI_F32 = 0,
+    SS_EPI_F32_ADD = 1,
+    SS_EPI_BIAS_LRELU_BF16 = 2,
+    SS_EPI_BIAS_F32 = 3
+} ss_gemm_epilogue;
+int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N, int32_t K,
+                     int32_t epi, void* C, int64_t ldc, const float* bias, float slope, int32_t splits,
+                     int32_t* err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

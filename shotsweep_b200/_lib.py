@@ -70,6 +70,7 @@ class SurfaceEstimate(ctypes.Structure):
                 ('status', ctypes.c_int32)]
 
 
+EPI_F32, EPI_F32_ADD, EPI_BIAS_LRELU_BF16, EPI_BIAS_F32 = 0, 1, 2, 3
 SURF_OK, SURF_NO_ONSETS, SURF_FEW_NEAR, SURF_SLOPE, SURF_FEW_SHOTS, SURF_UNRELIABLE, SURF_NONFINITE = range(7)
 MAX_CLUSTER = 16
 
@@ -122,6 +123,9 @@ _SIGNATURES = {
     'ss_f16_scaled': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_float, _P, _P]),
     'ss_velocity_targets': (ctypes.c_int32, [_P, ctypes.c_int64, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, _P, _P]),
+    'ss_gemm_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int64, _P, ctypes.c_float,
+                                      ctypes.c_int32, _P, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

@@ -16,7 +16,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 SOURCES = sorted((HERE / 'csrc').glob('*.cu'))
-HEADERS = [ROOT / 'include' / 'shotsweep.h', *sorted((HERE / 'csrc').glob('*.h'))]
+HEADERS = [ROOT / 'include' / 'shotsweep.h', *sorted((HERE / 'csrc').glob('*.h')), *sorted((HERE / 'csrc').glob('*.cuh'))]
 LIBRARY = HERE / 'libshotsweep.so'
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
