@@ -354,6 +354,43 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
                      int32_t epi, void* C, int64_t ldc, const float* bias, float slope, int32_t splits,
                      int32_t* err, void* stream);
 
+/* Convolution plumbing (NHWC BF16 activations).  conv[11] = {B, Hin, Win, Cin,
+ * KH, KW, stride_h, stride_w, pad_h, pad_w, up}: the input is read through a
+ * nearest-neighbour upsampling by `up`; Hout = (Hin*up + 2 pad_h - KH) / stride_h + 1
+ * (likewise W); column index k = (kh*KW + kw)*Cin + c.
+ *   ss_im2col_bf16        cols [pixels][Kc] (k >= KH*KW*Cin zero), or with
+ *                         `transposed` [KH*KW*Cin][ldt] (pixels innermost)
+ *   ss_col2im_lrelu_bf16  dpre[pixel][c] (row stride ldp) = leaky_relu'(y) x the
+ *                         sum of the column gradients dcols [pixels_out][Kc]
+ *                         that read input element (pixel, c); y: the input map
+ *   ss_transpose_bf16     out[c][r] = in[r][c]
+ *   ss_bias_grad_bf16     db[c] += sum over rows of dpre[row][c]
+ * Output head: crop [off, off+n)^2 of x [B][H][W][C], 3x3 convolution with
+ * zero padding, bias, tanh; head[6] = {B, H, W, C, off, n}; weights w[9][C].
+ *   ss_head_backward      dw += .., db += .., and dpre_x [B][H][W][C] =
+ *                         leaky_relu'(x) x the input gradient (zero outside the crop)
+ * ss_l1_tanh_loss         loss_sum += sum |pred - target|, dpre = sign(pred - target)/n x (1 - pred^2)
+ * ss_adamw                one AdamW step on float parameters (optional BF16 copy); the learning
+ *                         rate and the step counter (incremented first) are device values
+ * ss_gather_rows_f32      out[b][:] = src[ids[b]][:] (rows of `row` floats)
+ * ss_gathers_nhwc_bf16    network input: stored float16 gathers [n][S][T][X] of
+ *                         samples ids[0..B) as BF16 [B][T][X][S] / scale (3_train.py:198) */
+int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t transposed, int64_t ldt, void* cols,
+                       void* stream);
+int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
+                             void* dpre, int64_t ldp, void* stream);
+int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream);
+int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream);
+int32_t ss_head_forward(const void* x, const int32_t* head, const float* w, const float* bias, float* out, void* stream);
+int32_t ss_head_backward(const void* x, const int32_t* head, const float* w, const float* dpre, float slope, float* dw,
+                         float* db, void* dpre_x, void* stream);
+int32_t ss_l1_tanh_loss(const float* pred, const float* target, int64_t n, float* loss_sum, float* dpre, void* stream);
+int32_t ss_adamw(float* p, const float* grad, float* m, float* v, int64_t n, const float* lr, float b1, float b2,
+                 float eps, float wd, int32_t* step, void* p_bf16, void* stream);
+int32_t ss_gather_rows_f32(const float* src, const int32_t* ids, int32_t B, int64_t row, float* out, void* stream);
+int32_t ss_gathers_nhwc_bf16(const uint16_t* stored, const int32_t* ids, int32_t B, int32_t S, int32_t T, int32_t X,
+                             float scale, void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

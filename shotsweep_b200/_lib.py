@@ -126,6 +126,18 @@ _SIGNATURES = {
     'ss_gemm_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                                       ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int64, _P, ctypes.c_float,
                                       ctypes.c_int32, _P, _P]),
+    'ss_im2col_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _P, _P]),
+    'ss_col2im_lrelu_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, _P, ctypes.c_float, _P, ctypes.c_int64, _P]),
+    'ss_transpose_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int64, _P]),
+    'ss_bias_grad_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P, _P]),
+    'ss_head_forward': (ctypes.c_int32, [_P, _P, _P, _P, _P, _P]),
+    'ss_head_backward': (ctypes.c_int32, [_P, _P, _P, _P, ctypes.c_float, _P, _P, _P, _P]),
+    'ss_l1_tanh_loss': (ctypes.c_int32, [_P, _P, ctypes.c_int64, _P, _P, _P]),
+    'ss_adamw': (ctypes.c_int32, [_P, _P, _P, _P, ctypes.c_int64, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, _P, _P, _P]),
+    'ss_gather_rows_f32': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int64, _P, _P]),
+    'ss_gathers_nhwc_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_float, _P, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

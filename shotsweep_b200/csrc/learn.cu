@@ -206,6 +206,265 @@ int launch_gemm_bn(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const 
   }
 }
 
+
+// ---- convolution plumbing ----------------------------------------------------
+// Activations are NHWC BF16.  A convolution layer reads its input through an
+// optional nearest-neighbour upsampling by `up` (the decoder's x2 steps) and
+// has im2col column index k = (kh * KW + kw) * Cin + c.
+struct ConvGeom {
+  int B, Hin, Win, Cin, KH, KW, sh, sw, ph, pw, up, Hout, Wout;
+};
+
+__device__ __forceinline__ int64_t conv_src(const ConvGeom& g, int64_t m, int k) {
+  const int c = k % g.Cin, kk = k / g.Cin, kw = kk % g.KW, kh = kk / g.KW;
+  const int ox = static_cast<int>(m % g.Wout);
+  const int64_t t = m / g.Wout;
+  const int oy = static_cast<int>(t % g.Hout);
+  const int b = static_cast<int>(t / g.Hout);
+  const int uy = oy * g.sh - g.ph + kh, ux = ox * g.sw - g.pw + kw;
+  if (uy < 0 || ux < 0 || uy >= g.Hin * g.up || ux >= g.Win * g.up) return -1;
+  return ((static_cast<int64_t>(b) * g.Hin + uy / g.up) * g.Win + ux / g.up) * g.Cin + c;
+}
+
+__global__ void im2col_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int Kc, bf16* __restrict__ cols) {
+  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
+  const int64_t total = M * Kc;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int k = static_cast<int>(i % Kc);
+    const int64_t m = i / Kc;
+    const int64_t src = k < K ? conv_src(g, m, k) : -1;
+    cols[i] = src >= 0 ? x[src] : __float2bfloat16_rn(0.f);
+  }
+}
+
+// The same columns transposed, [Kc][ldt] (pixels innermost), for weight gradients.
+__global__ void im2col_t_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int64_t ldt, bf16* __restrict__ colst) {
+  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
+  const int64_t total = M * K;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t m = i % M;
+    const int k = static_cast<int>(i / M);
+    const int64_t src = conv_src(g, m, k);
+    colst[static_cast<int64_t>(k) * ldt + m] = src >= 0 ? x[src] : __float2bfloat16_rn(0.f);
+  }
+}
+
+// Column gradients back onto the input (the transpose of im2col, as a
+// gather: no atomics, deterministic), times the leaky-ReLU derivative of the
+// layer below, whose output y is the input here: dpre = dx * (y > 0 ? 1 : slope).
+__global__ void col2im_lrelu_kernel(const float* __restrict__ dcols, ConvGeom g, int Kc, const bf16* __restrict__ y,
+                                    float slope, bf16* __restrict__ dpre, int64_t ldp) {
+  const int64_t total = static_cast<int64_t>(g.B) * g.Hin * g.Win * g.Cin;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(i % g.Cin);
+    const int64_t pix = i / g.Cin;
+    const int ix = static_cast<int>(pix % g.Win);
+    const int64_t t = pix / g.Win;
+    const int iy = static_cast<int>(t % g.Hin);
+    const int b = static_cast<int>(t / g.Hin);
+    float acc = 0.f;
+    for (int uy = iy * g.up; uy < (iy + 1) * g.up; ++uy)
+      for (int kh = 0; kh < g.KH; ++kh) {
+        const int ty = uy + g.ph - kh;
+        if (ty < 0 || ty % g.sh) continue;
+        const int oy = ty / g.sh;
+        if (oy >= g.Hout) continue;
+        for (int ux = ix * g.up; ux < (ix + 1) * g.up; ++ux)
+          for (int kw = 0; kw < g.KW; ++kw) {
+            const int tx = ux + g.pw - kw;
+            if (tx < 0 || tx % g.sw) continue;
+            const int ox = tx / g.sw;
+            if (ox >= g.Wout) continue;
+            const int64_t m = (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout + ox;
+            acc += dcols[m * Kc + (kh * g.KW + kw) * g.Cin + c];
+          }
+      }
+    const float yv = __bfloat162float(y[i]);
+    dpre[pix * ldp + c] = __float2bfloat16_rn(yv > 0.f ? acc : slope * acc);
+  }
+}
+
+__global__ void transpose_bf16_kernel(const bf16* __restrict__ in, int64_t ld_in, int R, int C, bf16* __restrict__ out,
+                                      int64_t ld_out) {
+  __shared__ bf16 tile[32][33];
+  const int64_t r0 = static_cast<int64_t>(blockIdx.y) * 32, c0 = static_cast<int64_t>(blockIdx.x) * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int64_t r = r0 + j, c = c0 + threadIdx.x;
+    if (r < R && c < C) tile[j][threadIdx.x] = in[r * ld_in + c];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int64_t c = c0 + j, r = r0 + threadIdx.x;
+    if (r < R && c < C) out[c * ld_out + r] = tile[threadIdx.x][j];
+  }
+}
+
+// db[c] += sum over rows of dpre[row][c]
+__global__ void bias_grad_kernel(const bf16* __restrict__ dpre, int64_t ld, int64_t M, int C, float* __restrict__ db) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  float acc = 0.f;
+  for (int64_t m = blockIdx.y; m < M; m += gridDim.y) acc += __bfloat162float(dpre[m * ld + c]);
+  atomicAdd(db + c, acc);
+}
+
+// Output head: crop rows/cols [off, off+n) of x [B][H][W][C], 3x3 convolution
+// with zero padding, bias, tanh (the reference decoder's head on the cropped map).
+struct HeadGeom {
+  int B, H, W, C, off, n;
+};
+
+__global__ void head_forward_kernel(const bf16* __restrict__ x, HeadGeom g, const float* __restrict__ w,
+                                    const float* __restrict__ bias_dev, float* __restrict__ out) {
+  const float bias = *bias_dev;
+  const int64_t total = static_cast<int64_t>(g.B) * g.n * g.n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int xo = static_cast<int>(i % g.n), yo = static_cast<int>((i / g.n) % g.n);
+    const int b = static_cast<int>(i / (static_cast<int64_t>(g.n) * g.n));
+    float acc = bias;
+    for (int kh = 0; kh < 3; ++kh) {
+      const int yy = yo + kh - 1;
+      if (yy < 0 || yy >= g.n) continue;
+      for (int kw = 0; kw < 3; ++kw) {
+        const int xx = xo + kw - 1;
+        if (xx < 0 || xx >= g.n) continue;
+        const bf16* px = x + ((static_cast<int64_t>(b) * g.H + yy + g.off) * g.W + xx + g.off) * g.C;
+        const float* wk = w + (kh * 3 + kw) * g.C;
+        for (int c = 0; c < g.C; ++c) acc = fmaf(__bfloat162float(px[c]), wk[c], acc);
+      }
+    }
+    out[i] = tanhf(acc);
+  }
+}
+
+// L1 loss of tanh outputs: loss_sum += sum |p - t|; dpre = sign(p - t) / n * (1 - p^2).
+__global__ void l1_tanh_kernel(const float* __restrict__ p, const float* __restrict__ t, int64_t n, float inv_n,
+                               float* __restrict__ loss_sum, float* __restrict__ dpre) {
+  float acc = 0.f;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float d = p[i] - t[i];
+    acc += fabsf(d);
+    const float sg = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
+    dpre[i] = sg * inv_n * (1.f - p[i] * p[i]);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss_sum, acc);
+}
+
+// Head backward: weight / bias gradients (dw [9][C] += ..., db += ...) and the
+// input gradient on the uncropped map times the leaky-ReLU derivative of x.
+__global__ void head_wgrad_kernel(const bf16* __restrict__ x, HeadGeom g, const float* __restrict__ dpre,
+                                  float* __restrict__ dw, float* __restrict__ db) {
+  // one thread per (tap, channel); blocks split the pixels
+  const int j = threadIdx.x;               // tap * C + c, blockDim.x = 9 * C
+  const int tap = j / g.C, c = j % g.C, kh = tap / 3, kw = tap % 3;
+  const int64_t total = static_cast<int64_t>(g.B) * g.n * g.n;
+  float acc = 0.f, accb = 0.f;
+  for (int64_t i = blockIdx.x; i < total; i += gridDim.x) {
+    const int xo = static_cast<int>(i % g.n), yo = static_cast<int>((i / g.n) % g.n);
+    const int b = static_cast<int>(i / (static_cast<int64_t>(g.n) * g.n));
+    const float d = dpre[i];
+    if (j == 0) accb += d;
+    const int yy = yo + kh - 1, xx = xo + kw - 1;
+    if (yy < 0 || yy >= g.n || xx < 0 || xx >= g.n) continue;
+    acc = fmaf(d, __bfloat162float(x[((static_cast<int64_t>(b) * g.H + yy + g.off) * g.W + xx + g.off) * g.C + c]), acc);
+  }
+  atomicAdd(dw + j, acc);
+  if (j == 0) atomicAdd(db, accb);
+}
+
+__global__ void head_dgrad_kernel(const bf16* __restrict__ x, HeadGeom g, const float* __restrict__ dpre,
+                                  const float* __restrict__ w, float slope, bf16* __restrict__ dpre_x) {
+  const int64_t total = static_cast<int64_t>(g.B) * g.H * g.W * g.C;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(i % g.C);
+    const int64_t pix = i / g.C;
+    const int X = static_cast<int>(pix % g.W), Y = static_cast<int>((pix / g.W) % g.H);
+    const int b = static_cast<int>(pix / (static_cast<int64_t>(g.W) * g.H));
+    const int yy = Y - g.off, xx = X - g.off;
+    float acc = 0.f;
+    if (yy >= 0 && yy < g.n && xx >= 0 && xx < g.n)
+      for (int kh = 0; kh < 3; ++kh) {
+        const int yo = yy - kh + 1;
+        if (yo < 0 || yo >= g.n) continue;
+        for (int kw = 0; kw < 3; ++kw) {
+          const int xo = xx - kw + 1;
+          if (xo < 0 || xo >= g.n) continue;
+          acc = fmaf(dpre[(static_cast<int64_t>(b) * g.n + yo) * g.n + xo], w[(kh * 3 + kw) * g.C + c], acc);
+        }
+      }
+    const float yv = __bfloat162float(x[i]);
+    dpre_x[i] = __float2bfloat16_rn(yv > 0.f ? acc : slope * acc);
+  }
+}
+
+// AdamW (decoupled weight decay), then the BF16 copy used by the GEMMs.
+__global__ void step_inc_kernel(int* step) { *step += 1; }
+
+// lr and the step count live in device memory, so that a captured training
+// step replays with the current values.
+__global__ void adamw_kernel(float* __restrict__ p, const float* __restrict__ grad, float* __restrict__ m,
+                             float* __restrict__ v, int64_t n, const float* __restrict__ lr_dev, float b1, float b2,
+                             float eps, float wd, const int* __restrict__ step, bf16* __restrict__ p16) {
+  const float lr = *lr_dev;
+  const float c1 = 1.f - powf(b1, static_cast<float>(*step)), c2 = 1.f - powf(b2, static_cast<float>(*step));
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float gi = grad[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    float pi = p[i] * (1.f - lr * wd);
+    pi -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = pi;
+    if (p16) p16[i] = __float2bfloat16_rn(pi);
+  }
+}
+
+// Network input: stored float16 gathers [n][S][T][X] of the samples ids[0..B)
+// as BF16 NHWC [B][T][X][S] divided by the normalisation scale.
+__global__ void gathers_nhwc_kernel(const uint16_t* __restrict__ stored, const int* __restrict__ ids, int B, int S,
+                                    int T, int X, float scale, bf16* __restrict__ out) {
+  const int64_t total = static_cast<int64_t>(B) * T * X * S;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int s = static_cast<int>(i % S);
+    const int64_t tx = i / S;
+    const int x = static_cast<int>(tx % X);
+    const int64_t bt = tx / X;
+    const int t = static_cast<int>(bt % T);
+    const int b = static_cast<int>(bt / T);
+    const int64_t src = ((static_cast<int64_t>(ids[b]) * S + s) * T + t) * X + x;
+    const float v = __fdiv_rn(__half2float(__ushort_as_half(stored[src])), scale);
+    out[i] = __float2bfloat16_rn(v);
+  }
+}
+
+__global__ void gather_rows_kernel(const float* __restrict__ src, const int* __restrict__ ids, int B, int64_t row,
+                                   float* __restrict__ out) {
+  const int64_t total = static_cast<int64_t>(B) * row;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = src[static_cast<int64_t>(ids[i / row]) * row + i % row];
+}
+
+int grid_for_l(long long total) {
+  return static_cast<int>(std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 32)));
+}
+
+ConvGeom conv_geom(const int32_t* d) {
+  ConvGeom g{d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7], d[8], d[9], d[10], 0, 0};
+  g.Hout = (g.Hin * g.up + 2 * g.ph - g.KH) / g.sh + 1;
+  g.Wout = (g.Win * g.up + 2 * g.pw - g.KW) / g.sw + 1;
+  return g;
+}
 }  // namespace
 
 extern "C" {
@@ -245,6 +504,125 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
     case 128: return launch_gemm_bn<128>(epi, ta, tb, g, splits, st);
     default: return launch_gemm_bn<256>(epi, ta, tb, g, splits, st);
   }
+}
+
+// conv: {B, Hin, Win, Cin, KH, KW, sh, sw, ph, pw, up}; the output size follows.
+int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t transposed, int64_t ldt, void* cols,
+                       void* stream) {
+  ss_internal::clear_error();
+  if (!x || !conv || !cols) return fail(SS_ERR_INVALID, "bad arguments");
+  const ConvGeom g = conv_geom(conv);
+  const int K = g.KH * g.KW * g.Cin;
+  if (g.Hout < 1 || g.Wout < 1 || g.up < 1 || g.sh < 1 || g.sw < 1 || Kc < K) return fail(SS_ERR_INVALID, "bad convolution");
+  const long long M = static_cast<long long>(g.B) * g.Hout * g.Wout;
+  if (transposed && ldt < M) return fail(SS_ERR_INVALID, "transposed columns need ldt >= pixels");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (transposed)
+    im2col_t_kernel<<<grid_for_l(M * K), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, ldt, static_cast<bf16*>(cols));
+  else
+    im2col_kernel<<<grid_for_l(M * Kc), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, Kc, static_cast<bf16*>(cols));
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
+                             void* dpre, int64_t ldp, void* stream) {
+  ss_internal::clear_error();
+  if (!dcols || !conv || !y || !dpre) return fail(SS_ERR_INVALID, "bad arguments");
+  const ConvGeom g = conv_geom(conv);
+  if (ldp < g.Cin) return fail(SS_ERR_INVALID, "ldp < channels");
+  const long long total = static_cast<long long>(g.B) * g.Hin * g.Win * g.Cin;
+  col2im_lrelu_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      dcols, g, Kc, static_cast<const bf16*>(y), slope, static_cast<bf16*>(dpre), ldp);
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream) {
+  ss_internal::clear_error();
+  if (!in || !out || R < 1 || C < 1 || ld_in < C || ld_out < R) return fail(SS_ERR_INVALID, "bad arguments");
+  dim3 grid((C + 31) / 32, (R + 31) / 32);
+  transpose_bf16_kernel<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out), ld_out);
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream) {
+  ss_internal::clear_error();
+  if (!dpre || !db || M < 1 || C < 1 || ld < C) return fail(SS_ERR_INVALID, "bad arguments");
+  dim3 grid((C + 127) / 128, static_cast<unsigned>(std::min<long long>(M, 512)));
+  bias_grad_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(dpre), ld, M, C, db);
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+// head: {B, H, W, C, off, n}
+int32_t ss_head_forward(const void* x, const int32_t* head, const float* w, const float* bias, float* out, void* stream) {
+  ss_internal::clear_error();
+  if (!x || !head || !w || !bias || !out) return fail(SS_ERR_INVALID, "bad arguments");
+  const HeadGeom g{head[0], head[1], head[2], head[3], head[4], head[5]};
+  if (g.off < 0 || g.off + g.n > g.H || g.off + g.n > g.W) return fail(SS_ERR_INVALID, "crop outside the map");
+  const long long total = static_cast<long long>(g.B) * g.n * g.n;
+  head_forward_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(x), g,
+                                                                                       w, bias, out);
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_head_backward(const void* x, const int32_t* head, const float* w, const float* dpre, float slope, float* dw,
+                         float* db, void* dpre_x, void* stream) {
+  ss_internal::clear_error();
+  if (!x || !head || !w || !dpre || !dw || !db || !dpre_x) return fail(SS_ERR_INVALID, "bad arguments");
+  const HeadGeom g{head[0], head[1], head[2], head[3], head[4], head[5]};
+  if (9 * g.C > 1024) return fail(SS_ERR_UNSUPPORTED, "head with more than 113 channels");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  head_wgrad_kernel<<<296, 9 * g.C, 0, st>>>(static_cast<const bf16*>(x), g, dpre, dw, db);
+  const long long total = static_cast<long long>(g.B) * g.H * g.W * g.C;
+  head_dgrad_kernel<<<grid_for_l(total), 256, 0, st>>>(static_cast<const bf16*>(x), g, dpre, w, slope,
+                                                        static_cast<bf16*>(dpre_x));
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_l1_tanh_loss(const float* pred, const float* target, int64_t n, float* loss_sum, float* dpre, void* stream) {
+  ss_internal::clear_error();
+  if (!pred || !target || !loss_sum || !dpre || n < 1) return fail(SS_ERR_INVALID, "bad arguments");
+  l1_tanh_kernel<<<grid_for_l(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(pred, target, n, 1.f / n, loss_sum, dpre);
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_adamw(float* p, const float* grad, float* m, float* v, int64_t n, const float* lr, float b1, float b2,
+                 float eps, float wd, int32_t* step, void* p_bf16, void* stream) {
+  ss_internal::clear_error();
+  if (!p || !grad || !m || !v || !lr || !step || n < 1) return fail(SS_ERR_INVALID, "bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  step_inc_kernel<<<1, 1, 0, st>>>(step);
+  adamw_kernel<<<grid_for_l(n), 256, 0, st>>>(p, grad, m, v, n, lr, b1, b2, eps, wd, step, static_cast<bf16*>(p_bf16));
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_gather_rows_f32(const float* src, const int32_t* ids, int32_t B, int64_t row, float* out, void* stream) {
+  ss_internal::clear_error();
+  if (!src || !ids || !out || B < 1 || row < 1) return fail(SS_ERR_INVALID, "bad arguments");
+  const long long total = static_cast<long long>(B) * row;
+  gather_rows_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(src, ids, B, row, out);
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_gathers_nhwc_bf16(const uint16_t* stored, const int32_t* ids, int32_t B, int32_t S, int32_t T, int32_t X,
+                             float scale, void* out, void* stream) {
+  ss_internal::clear_error();
+  if (!stored || !ids || !out || B < 1 || S < 1 || T < 1 || X < 1) return fail(SS_ERR_INVALID, "bad arguments");
+  if (!std::isfinite(scale) || !(scale > 0.f)) return fail(SS_ERR_INVALID, "Gather normalization scale must be finite and positive");
+  const long long total = static_cast<long long>(B) * S * T * X;
+  gathers_nhwc_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(stored, ids, B, S, T, X, scale,
+                                                                                       static_cast<bf16*>(out));
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
 }
 
 }  // extern "C"
