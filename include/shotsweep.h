@@ -391,6 +391,30 @@ int32_t ss_gather_rows_f32(const float* src, const int32_t* ids, int32_t B, int6
 int32_t ss_gathers_nhwc_bf16(const uint16_t* stored, const int32_t* ids, int32_t B, int32_t S, int32_t T, int32_t X,
                              float scale, void* out, void* stream);
 
+/* ---- L-BFGS full-waveform inversion, batched over models (the reference's
+ * archive/toy/slopes/fwi.py:130-164 for many models at once; one CTA per model) ----
+ * ss_fwi_precondition  out[m] = mute * smooth_x(smooth_z(mute * sum_s grads[m][s]))
+ *                      (fwi.py:142-143; Gaussian of sigma `smooth` cells, radius
+ *                      int(3 sigma) + 1, edge padding, slopes.py:20-26)
+ * ss_fwi_misfit        J[m] = 0.5 sum (sim - obs)^2 over per_model values (float64)
+ * ss_lbfgs_direction   d[m] from g[m] and the model's last count[m] (s, y) pairs
+ *                      (slots next[m]-count[m] .. next[m]-1 of S, Y [B][mem][n]);
+ *                      first step scaled to max |d| = cap, steepest descent of
+ *                      max |d| = cap (and count[m] = 0) when g.d >= 0; gd[m] = g.d
+ * ss_fwi_trial         vt[m] = clip(v[m] + step[m] d[m], lo, hi) where mask[m]
+ * ss_lbfgs_push        where accept[m]: push (vt - v, gn - g) if s.y > 1e-12, then
+ *                      v = vt, g = gn */
+int32_t ss_fwi_precondition(const float* grads, int32_t B, int32_t S, int32_t nz, int32_t nx, float smooth, float* out,
+                            void* stream);
+int32_t ss_fwi_misfit(const float* sim, const float* obs, int32_t B, int64_t per_model, double* J, void* stream);
+int32_t ss_lbfgs_direction(const float* g, const float* S, const float* Y, int32_t* count, const int32_t* next,
+                           const int32_t* active, int32_t B, int32_t n, int32_t mem, float cap, float* d, double* gd,
+                           void* stream);
+int32_t ss_fwi_trial(const float* v, const float* d, const float* step, const int32_t* mask, int32_t B, int32_t n,
+                     float lo, float hi, float* vt, void* stream);
+int32_t ss_lbfgs_push(float* v, const float* vt, float* g, const float* gn, float* S, float* Y, int32_t* count,
+                      int32_t* next, const int32_t* accept, int32_t B, int32_t n, int32_t mem, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

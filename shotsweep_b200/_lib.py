@@ -138,6 +138,15 @@ _SIGNATURES = {
     'ss_gather_rows_f32': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int64, _P, _P]),
     'ss_gathers_nhwc_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                               ctypes.c_float, _P, _P]),
+    'ss_fwi_precondition': (ctypes.c_int32, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_float, _P, _P]),
+    'ss_fwi_misfit': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int64, _P, _P]),
+    'ss_lbfgs_direction': (ctypes.c_int32, [_P, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_float, _P, _P, _P]),
+    'ss_fwi_trial': (ctypes.c_int32, [_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float,
+                                      _P, _P]),
+    'ss_lbfgs_push': (ctypes.c_int32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_int32, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

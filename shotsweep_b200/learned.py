@@ -1,0 +1,156 @@
+"""Learned proposal + FWI: train on simulator gathers, propose, accept by forward misfit, refine by L-BFGS.
+
+    res = run(n_train=20000, n_test=256, steps=6000, iters=50)
+
+1. Training data: `n_train` seeded models from the synthetic families (an equal mix of
+   layered, curved, faulted and textured), their gathers simulated by the library's
+   forward kernel and kept on the device in the stored float16 form sign(g) log1p(|g|)
+   (3_train.py:157); the normalisation scale is the largest stored magnitude (3_train.py:513).
+2. Training: ``proposal.ProposalNet`` with AdamW (lr 5e-4 with cosine decay, weight decay
+   1e-4), L1 loss on (v - 3000) / 1500, batches drawn from a seeded permutation; one training
+   step is one CUDA-graph replay.
+3. Held-out models (`n_test`, other seeds): the network's velocity proposal, and the medium
+   background (surface velocity from the first-arrival picker + 1.0 x the training depth trend,
+   background.py:97-99; the training models' mean surface velocity where the picker refuses).
+4. Acceptance by forward misfit: each model starts FWI from the proposal if its data misfit is
+   below the background's, otherwise from the background (the fallback is plain FWI).
+5. ``fwi.BatchFWI`` from both starts for `iters` L-BFGS iterations; the time-to-misfit is the
+   wall time the learned start (inference and acceptance included) needs to reach the final
+   total misfit of plain FWI from the background, against plain FWI's own wall time.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import background as BG
+from . import engine, gpu, synth, train_inputs as TI
+from .fwi import BatchFWI
+from .proposal import OUT, ProposalNet
+
+
+def simulate_stored(eng, models, w, chunk=1000):
+    """Stored float16 gathers [n, 5, 1000, 70] (device) of models [n, 70, 70]."""
+    out = torch.empty(len(models), eng.g.n_shots, eng.g.nt, eng.g.nx, dtype=torch.float16, device=eng.device)
+    for a in range(0, len(models), chunk):
+        g = eng.forward(torch.tensor(models[a:a + chunk], dtype=torch.float32, device=eng.device), w)
+        out[a:a + len(g)] = TI.stored_gathers(g)
+    eng.status()
+    return out
+
+
+def train(net, stored, targets, scale, steps, lr=5e-4, seed=0, log_every=500, log=None):
+    """`steps` AdamW steps on batches of net.B samples; returns the loss of every `log_every`-th step."""
+    n = stored.shape[0]
+    rng = np.random.default_rng([seed, 5])
+    perm = torch.tensor(np.concatenate([rng.permutation(n) for _ in range(math.ceil(steps * net.B / n) + 1)]),
+                        dtype=torch.int32, device=net.dev)
+    net.ids.copy_(perm[:net.B])
+    net.train_step(stored, scale, targets)          # warm-up outside capture (attributes, tensor maps)
+    torch.cuda.synchronize(net.dev)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        net.train_step(stored, scale, targets)
+    losses = []
+    for s in range(1, steps):
+        net.ids.copy_(perm[s * net.B:(s + 1) * net.B])
+        net.lr.fill_(lr * 0.5 * (1 + math.cos(math.pi * s / steps)))
+        graph.replay()
+        if s % log_every == 0 or s == steps - 1:
+            losses.append((s, net.loss_sum.item() / (net.B * OUT * OUT)))
+            if log:
+                log(s, losses[-1][1])
+    net.check()
+    del graph
+    return losses
+
+
+def predict(net, stored, scale):
+    """Velocities [n, 70, 70] (float32, device) proposed for every stored sample."""
+    n = stored.shape[0]
+    out = torch.empty(n, OUT, OUT, dtype=torch.float32, device=net.dev)
+    for a in range(0, n, net.B):
+        ids = torch.arange(a, a + net.B, dtype=torch.int32, device=net.dev).clamp_max(n - 1)
+        net.ids.copy_(ids)
+        net.load_batch(stored, scale)
+        pred = net.forward()
+        k = min(net.B, n - a)
+        out[a:a + k] = pred[:k] * 1500.0 + 3000.0
+    return out
+
+
+def medium_backgrounds(gathers, trend, fallback_vs, device):
+    """Medium (rho = 1.0) backgrounds from picked surface velocities; the fallback where the picker refuses."""
+    est = BG.surface_estimates(gathers)
+    vs = np.array([e.velocity if e.status == 0 else fallback_vs for e in est])
+    return BG.backgrounds(vs, trend, rhos=(1.0,), device=device)[:, 0], vs, np.array([e.status for e in est])
+
+
+def norm_mae(v, truth):
+    """Mean absolute error of velocities normalised to [-1, 1] (the reference's metric, fwi.py norm/metrics)."""
+    a = (np.clip(v, 1500, 4500) - 1500) / 3000 * 2 - 1
+    b = (np.clip(truth, 1500, 4500) - 1500) / 3000 * 2 - 1
+    return float(np.abs(a - b).mean())
+
+
+def run(n_train=20000, n_test=256, steps=6000, batch=64, iters=50, seed=0, train_tag=101, test_tag=202, log=print):
+    dev = torch.device('cuda', torch.cuda.current_device())
+    sim = gpu.Sim(device=dev)
+    eng = sim.engine
+    w = engine.scaled_wavelet(gpu.RICKER, dev)
+    res = {}
+    t0 = time.perf_counter()
+    train_models = synth.population(n_train, tag=train_tag)
+    test_models = synth.population(n_test, tag=test_tag)
+    stored = simulate_stored(eng, train_models, w)
+    scale = float(stored.abs().max().item())
+    targets = TI.targets(torch.tensor(train_models, device=dev)).contiguous()
+    res['data_seconds'] = time.perf_counter() - t0
+    net = ProposalNet(batch, device=dev, seed=seed)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    res['losses'] = train(net, stored, targets, scale, steps, seed=seed,
+                          log=(lambda s, l: log(f'step {s}: L1 {l:.4f}')) if log else None)
+    torch.cuda.synchronize(dev)
+    res['train_seconds'] = time.perf_counter() - t1
+    res['train_steps_per_s'] = steps / res['train_seconds']
+    del stored
+    # held-out models
+    obs = eng.forward(torch.tensor(test_models, device=dev), w)
+    trend = BG.depth_trend(train_models)
+    fallback_vs = float(train_models[:, 0].mean())
+    bg, vs, picked = medium_backgrounds(obs, trend, fallback_vs, dev)
+    res['picker_refused'] = int((picked != 0).sum())
+    fwi = BatchFWI(eng, w, obs)
+    J_bg = fwi.misfit(bg.reshape(n_test, -1).contiguous(), torch.empty(n_test, dtype=torch.float64, device=dev)).cpu().numpy()
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    test_stored = TI.stored_gathers(obs)
+    prop = predict(net, test_stored, scale)
+    J_prop = fwi.misfit(prop.reshape(n_test, -1).contiguous(),
+                        torch.empty(n_test, dtype=torch.float64, device=dev)).cpu().numpy()
+    use = J_prop < J_bg
+    start = torch.where(torch.tensor(use, device=dev)[:, None, None], prop, bg)
+    torch.cuda.synchronize(dev)
+    propose_s = time.perf_counter() - t2
+    res.update(accepted=int(use.sum()), J_background=float(J_bg.sum()), J_proposal=float(J_prop.sum()),
+               propose_seconds=propose_s,
+               mae_background=norm_mae(bg.cpu().numpy(), test_models),
+               mae_proposal=norm_mae(prop.cpu().numpy(), test_models))
+    v_plain, h_plain = BatchFWI(eng, w, obs).run(bg, iters)
+    v_learn, h_learn = BatchFWI(eng, w, obs).run(start, iters)
+    plain_total = [float(h[1].sum()) for h in h_plain]
+    learn_total = [float(h[1].sum()) for h in h_learn]
+    target = plain_total[-1]
+    t_plain = h_plain[-1][0]
+    reach = next((propose_s + h[0] for h, J in zip(h_learn, learn_total) if J <= target), None)
+    res.update(plain_final_misfit=target, learned_final_misfit=learn_total[-1], plain_seconds=t_plain,
+               learned_seconds=h_learn[-1][0] + propose_s, learned_time_to_plain_misfit=reach,
+               time_ratio=None if reach is None else reach / t_plain,
+               plain_misfit_curve=plain_total, learned_misfit_curve=learn_total,
+               mae_plain_fwi=norm_mae(v_plain.cpu().numpy(), test_models),
+               mae_learned_fwi=norm_mae(v_learn.cpu().numpy(), test_models))
+    return res
