@@ -66,7 +66,11 @@ def parse():
     ap.add_argument('--impl', choices=('ours', 'reference'), default='ours')
     ap.add_argument('--models', type=int, default=N_MODELS, help='velocity models per GPU')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--workload', choices=('openfwi', 'uneven', 'process'), default='openfwi')
+    ap.add_argument('--workload', choices=('openfwi', 'uneven', 'process', 'learned'), default='openfwi')
+    ap.add_argument('--train-models', type=int, default=20000, help='learned workload: training models')
+    ap.add_argument('--train-steps', type=int, default=6000, help='learned workload: AdamW steps (batch 64)')
+    ap.add_argument('--test-models', type=int, default=256, help='learned workload: held-out models')
+    ap.add_argument('--fwi-iters', type=int, default=50, help='learned workload: L-BFGS iterations')
     ap.add_argument('--solves', type=int, default=2000, help='uneven workload: solves per GPU')
     ap.add_argument('--schedule', type=int, default=-1, choices=(-1, 0, 1, 2),
                     help='uneven workload: stream schedule (-1: autotuned)')
@@ -518,6 +522,42 @@ def run_process(args):
     return 0
 
 
+def run_learned(args):
+    """Learned proposal + FWI vs plain FWI on held-out models: time-to-misfit (the reference's second metric)."""
+    import torch
+    from shotsweep_b200 import dist as D
+    from shotsweep_b200 import learned
+    rank, world, local = D.init('nccl' if args.gpus > 1 else 'gloo', timeout_s=1800)
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    with ClockSampler(bus_id(dev)) as clk:
+        res = learned.run(n_train=args.train_models, n_test=args.test_models, steps=args.train_steps,
+                          iters=args.fwi_iters, seed=rank, log=None)
+    if rank == 0:
+        print(json.dumps({
+            'metric': 'time-to-misfit: learned-proposal FWI to reach plain FWI\'s final data misfit, / plain FWI time',
+            'value': res['time_ratio'], 'unit': 'fraction of plain FWI wall time', 'n_gpus': world,
+            'steps': args.fwi_iters, 'warmup': 0, 'higher_is_better': False, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'bf16 network (f32 accumulate), f32 physics',
+            'data': 'synthetic: seeded models of the four families, gathers simulated by this library',
+            'config': {'workload': f'{args.train_models} training models, {args.train_steps} AdamW steps of 64, '
+                                   f'{args.test_models} held-out models, {args.fwi_iters} L-BFGS iterations each',
+                       'parameters': 2961536},
+            'plain_fwi_seconds': res['plain_seconds'], 'learned_time_to_plain_misfit_s': res['learned_time_to_plain_misfit'],
+            'propose_seconds': res['propose_seconds'], 'train_seconds': res['train_seconds'],
+            'train_steps_per_s': res['train_steps_per_s'], 'data_seconds': res['data_seconds'],
+            'misfit': {'background': res['J_background'], 'proposal': res['J_proposal'],
+                       'plain_final': res['plain_final_misfit'], 'learned_final': res['learned_final_misfit']},
+            'normalised_mae': {'background': res['mae_background'], 'proposal': res['mae_proposal'],
+                               'plain_fwi': res['mae_plain_fwi'], 'learned_fwi': res['mae_learned_fwi']},
+            'accepted_proposals': res['accepted'], 'picker_refused': res['picker_refused'],
+            'final_train_l1': res['losses'][-1][1] if res['losses'] else None,
+            'clocks': clk.summary(),
+        }), flush=True)
+    D.finish()
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 0 or args.steps < 1:
@@ -528,6 +568,8 @@ def main():
         return run_uneven(args)
     if args.workload == 'process':
         return run_process(args)
+    if args.workload == 'learned':
+        return run_learned(args)
     return run_ours(args)
 
 
