@@ -238,6 +238,25 @@ __global__ void im2col_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int
   }
 }
 
+// 8 channels (16 bytes) per thread where Cin % 8 == 0 (then K == Kc).
+__global__ void im2col_vec8_kernel(const bf16* __restrict__ x, ConvGeom g, bf16* __restrict__ cols) {
+  const int chunks = g.Cin / 8, taps = g.KH * g.KW;
+  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
+  const int64_t total = M * taps * chunks;
+  const int64_t K = static_cast<int64_t>(taps) * g.Cin;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int ch = static_cast<int>(i % chunks);
+    const int64_t mt = i / chunks;
+    const int tap = static_cast<int>(mt % taps);
+    const int64_t m = mt / taps;
+    const int64_t src = conv_src(g, m, tap * g.Cin + ch * 8);
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (src >= 0) v = *reinterpret_cast<const uint4*>(x + src);
+    *reinterpret_cast<uint4*>(cols + m * K + tap * g.Cin + ch * 8) = v;
+  }
+}
+
 // The same columns transposed, [Kc][ldt] (pixels innermost), for weight gradients.
 __global__ void im2col_t_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int64_t ldt, bf16* __restrict__ colst) {
   const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
@@ -248,6 +267,56 @@ __global__ void im2col_t_kernel(const bf16* __restrict__ x, ConvGeom g, int K, i
     const int k = static_cast<int>(i / M);
     const int64_t src = conv_src(g, m, k);
     colst[static_cast<int64_t>(k) * ldt + m] = src >= 0 ? x[src] : __float2bfloat16_rn(0.f);
+  }
+}
+
+// 4 channels per thread (Cin % 4 == 0 and a row stride Kc % 4 == 0): float4 gathers.
+__global__ void col2im_lrelu_vec4_kernel(const float* __restrict__ dcols, ConvGeom g, int Kc, const bf16* __restrict__ y,
+                                         float slope, bf16* __restrict__ dpre, int64_t ldp) {
+  const int chunks = g.Cin / 4;
+  const int64_t total = static_cast<int64_t>(g.B) * g.Hin * g.Win * chunks;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(i % chunks) * 4;
+    const int64_t pix = i / chunks;
+    const int ix = static_cast<int>(pix % g.Win);
+    const int64_t t = pix / g.Win;
+    const int iy = static_cast<int>(t % g.Hin);
+    const int b = static_cast<int>(t / g.Hin);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int uy = iy * g.up; uy < (iy + 1) * g.up; ++uy)
+      for (int kh = 0; kh < g.KH; ++kh) {
+        const int ty = uy + g.ph - kh;
+        if (ty < 0 || ty % g.sh) continue;
+        const int oy = ty / g.sh;
+        if (oy >= g.Hout) continue;
+        for (int ux = ix * g.up; ux < (ix + 1) * g.up; ++ux)
+          for (int kw = 0; kw < g.KW; ++kw) {
+            const int tx = ux + g.pw - kw;
+            if (tx < 0 || tx % g.sw) continue;
+            const int ox = tx / g.sw;
+            if (ox >= g.Wout) continue;
+            const int64_t m = (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout + ox;
+            const float4 d = *reinterpret_cast<const float4*>(dcols + m * Kc + (kh * g.KW + kw) * g.Cin + c);
+            acc.x += d.x;
+            acc.y += d.y;
+            acc.z += d.z;
+            acc.w += d.w;
+          }
+      }
+    const float a[4] = {acc.x, acc.y, acc.z, acc.w};
+    bf16 o[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float yv = __bfloat162float(y[pix * g.Cin + c + j]);
+      o[j] = __float2bfloat16_rn(yv > 0.f ? a[j] : slope * a[j]);
+    }
+    bf16* dst = dpre + pix * ldp + c;
+    if ((ldp & 3) == 0) {
+      *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(o);
+    } else {
+      for (int j = 0; j < 4; ++j) dst[j] = o[j];
+    }
   }
 }
 
@@ -519,6 +588,9 @@ int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t t
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (transposed)
     im2col_t_kernel<<<grid_for_l(M * K), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, ldt, static_cast<bf16*>(cols));
+  else if (g.Cin % 8 == 0 && Kc == K && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+           (reinterpret_cast<uintptr_t>(cols) & 15) == 0)
+    im2col_vec8_kernel<<<grid_for_l(M * K / 8), 256, 0, st>>>(static_cast<const bf16*>(x), g, static_cast<bf16*>(cols));
   else
     im2col_kernel<<<grid_for_l(M * Kc), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, Kc, static_cast<bf16*>(cols));
   SS_TRY_CUDA(cudaGetLastError());
@@ -532,8 +604,14 @@ int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc
   const ConvGeom g = conv_geom(conv);
   if (ldp < g.Cin) return fail(SS_ERR_INVALID, "ldp < channels");
   const long long total = static_cast<long long>(g.B) * g.Hin * g.Win * g.Cin;
-  col2im_lrelu_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      dcols, g, Kc, static_cast<const bf16*>(y), slope, static_cast<bf16*>(dpre), ldp);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (g.Cin % 4 == 0 && Kc % 4 == 0 && (reinterpret_cast<uintptr_t>(dcols) & 15) == 0 &&
+      (reinterpret_cast<uintptr_t>(dpre) & 7) == 0)
+    col2im_lrelu_vec4_kernel<<<grid_for_l(total / 4), 256, 0, st>>>(dcols, g, Kc, static_cast<const bf16*>(y), slope,
+                                                                     static_cast<bf16*>(dpre), ldp);
+  else
+    col2im_lrelu_kernel<<<grid_for_l(total), 256, 0, st>>>(dcols, g, Kc, static_cast<const bf16*>(y), slope,
+                                                           static_cast<bf16*>(dpre), ldp);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }

@@ -1,6 +1,12 @@
-"""Small fixed workload for profiling the solve kernels with ncu.
+"""Small fixed workloads for profiling with ncu.
 
     python -m shotsweep_b200.profiling [n_models]
+    python -m shotsweep_b200.profiling learned [batch]
+
+The second form: `batch` simulated models (default 64), three training steps of the learned
+proposal (warm-up), then five timed steps; each step launches the network's 38 tensor-core
+GEMMs in the same order (13 forward, then per layer from the top the weight gradient and,
+below the first layer, the input gradient).
 
 Runs, on cuda:0, with `n_models` seeded synthetic models (default 9, i.e.
 45 solves, one round of three-CTA clusters on a B200):
@@ -42,5 +48,33 @@ def main(n_models=9):
           f'images {ev[2].elapsed_time(ev[3]):.3f} ms')
 
 
+def learned(batch=64):
+    from . import train_inputs as TI
+    from .proposal import ProposalNet
+    eng = engine.Engine(engine.geometry())
+    dev = eng.device
+    models = synth.population(batch, tag=7)
+    g = eng.forward(torch.tensor(models, device=dev), engine.scaled_wavelet(gpu.RICKER, dev))
+    stored = TI.stored_gathers(g)
+    scale = float(stored.abs().max().item())
+    y = TI.targets(torch.tensor(models, device=dev))
+    net = ProposalNet(batch, device=dev)
+    net.ids.copy_(torch.arange(batch, dtype=torch.int32))
+    for _ in range(3):
+        net.train_step(stored, scale, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        net.train_step(stored, scale, y)
+    e1.record()
+    torch.cuda.synchronize()
+    net.check()
+    print(f'batch={batch} training step {e0.elapsed_time(e1) / 5:.3f} ms, L1 {net.loss_sum.item() / (batch * 4900):.4f}')
+
+
 if __name__ == '__main__':
-    main(int(sys.argv[1]) if len(sys.argv) > 1 else 9)
+    if len(sys.argv) > 1 and sys.argv[1] == 'learned':
+        learned(int(sys.argv[2]) if len(sys.argv) > 2 else 64)
+    else:
+        main(int(sys.argv[1]) if len(sys.argv) > 1 else 9)

@@ -152,17 +152,16 @@ class ProposalNet:
         B = self.B
         self.x0 = torch.empty(B * T_IN * X_IN * S_IN, **bf)
         self.y = []
-        max_cols = max_colst = max_dcols = max_wt = max_dpret = 1
+        self.cols = []       # each convolution's im2col columns, kept from forward to backward
+        max_colst = max_dcols = max_wt = max_dpret = 1
         for L, (hi, wi, ho, wo, K, Kc, N) in zip(LAYERS, self.shapes):
             M = B * (ho * wo if L.kind != 'fc' else 1)
             self.y.append(torch.empty(M * N, **bf))
-            if L.kind == 'conv':
-                max_cols = max(max_cols, M * Kc)
+            self.cols.append(torch.empty(M * Kc, **bf) if L.kind == 'conv' else None)
             max_colst = max(max_colst, K * round8(M))
             max_dcols = max(max_dcols, M * K)
             max_wt = max(max_wt, K * round8(N))
             max_dpret = max(max_dpret, N * round8(M))
-        self.cols = torch.empty(max_cols, **bf)
         self.colst = torch.empty(max_colst, **bf)
         self.dcols = torch.empty(max_dcols, **f32)
         self.wt = torch.empty(max_wt, **bf)
@@ -222,9 +221,9 @@ class ProposalNet:
             hi, wi, ho, wo, K, Kc, N = self.shapes[i]
             M = self.B * (ho * wo if L.kind != 'fc' else 1)
             if L.kind == 'conv':
-                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols),
+                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols[i]),
                                                  self._stream()), 'ss_im2col_bf16')
-                A, lda = self.cols, Kc
+                A, lda = self.cols[i], Kc
             else:
                 A, lda = x, K
             self._gemm(A, lda, self.weight16(i), Kc, M, N, K, _lib.EPI_BIAS_LRELU_BF16, self.y[i], N,
@@ -258,12 +257,9 @@ class ProposalNet:
             M8 = round8(M)
             _lib.check(self.L.ss_transpose_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self.dpret), M8, self._stream()),
                        'ss_transpose_bf16')
-            if L.kind == 'conv':
-                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 1, M8, _lib.ptr(self.colst),
-                                                 self._stream()), 'ss_im2col_bf16')
-            else:
-                _lib.check(self.L.ss_transpose_bf16(_lib.ptr(x), K, M, K, _lib.ptr(self.colst), M8, self._stream()),
-                           'ss_transpose_bf16')
+            src, lds = (self.cols[i], Kc) if L.kind == 'conv' else (x, K)   # forward columns, or the input itself
+            _lib.check(self.L.ss_transpose_bf16(_lib.ptr(src), lds, M, K, _lib.ptr(self.colst), M8, self._stream()),
+                       'ss_transpose_bf16')
             self._gemm(self.dpret, M8, self.colst, M8, N, K, M, _lib.EPI_F32_ADD,
                        self._view(self.grads, L.name + '.w'), Kc)
             if i == 0:
