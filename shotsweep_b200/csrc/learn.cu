@@ -120,6 +120,38 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       tmem_ld16(taddr + (static_cast<uint32_t>(q * 32) << 16) + c, v);
       if (row >= g.M) continue;
       const long long off = static_cast<long long>(row) * g.ldc;
+      const int cbase = n0 + c;
+      // whole 16-column chunks with aligned rows: vector stores
+      if (cbase + 16 <= g.N && (EPI == SS_EPI_BIAS_LRELU_BF16 ? (g.ldc % 8 == 0) : (g.ldc % 4 == 0))) {
+        if (EPI == SS_EPI_BIAS_LRELU_BF16) {
+          __align__(16) bf16 o[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            float x = v[j] + (g.bias ? g.bias[cbase + j] : 0.f);
+            o[j] = __float2bfloat16_rn(x > 0.f ? x : g.slope * x);
+          }
+          uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(g.c) + off + cbase);
+          dst[0] = reinterpret_cast<const uint4*>(o)[0];
+          dst[1] = reinterpret_cast<const uint4*>(o)[1];
+        } else {
+          float4* dst = reinterpret_cast<float4*>(static_cast<float*>(g.c) + off + cbase);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            float4 q = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            if (EPI == SS_EPI_BIAS_F32 && g.bias) {
+              q.x += g.bias[cbase + 4 * j];
+              q.y += g.bias[cbase + 4 * j + 1];
+              q.z += g.bias[cbase + 4 * j + 2];
+              q.w += g.bias[cbase + 4 * j + 3];
+            }
+            if (EPI == SS_EPI_F32_ADD)
+              atomicAdd(dst + j, q);
+            else
+              dst[j] = q;
+          }
+        }
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int col = n0 + c + j;
@@ -432,16 +464,25 @@ __global__ void head_wgrad_kernel(const bf16* __restrict__ x, HeadGeom g, const 
   // one thread per (tap, channel); blocks split the pixels
   const int j = threadIdx.x;               // tap * C + c, blockDim.x = 9 * C
   const int tap = j / g.C, c = j % g.C, kh = tap / 3, kw = tap % 3;
-  const int64_t total = static_cast<int64_t>(g.B) * g.n * g.n;
+  const int total = g.B * g.n * g.n;       // checked < 2^31 on the host
+  const int per = (total + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(i0 + per, total);
   float acc = 0.f, accb = 0.f;
-  for (int64_t i = blockIdx.x; i < total; i += gridDim.x) {
-    const int xo = static_cast<int>(i % g.n), yo = static_cast<int>((i / g.n) % g.n);
-    const int b = static_cast<int>(i / (static_cast<int64_t>(g.n) * g.n));
+  int xo = i0 % g.n, yo = (i0 / g.n) % g.n, b = i0 / (g.n * g.n);
+  for (int i = i0; i < i1; ++i) {
     const float d = dpre[i];
     if (j == 0) accb += d;
     const int yy = yo + kh - 1, xx = xo + kw - 1;
-    if (yy < 0 || yy >= g.n || xx < 0 || xx >= g.n) continue;
-    acc = fmaf(d, __bfloat162float(x[((static_cast<int64_t>(b) * g.H + yy + g.off) * g.W + xx + g.off) * g.C + c]), acc);
+    if (yy >= 0 && yy < g.n && xx >= 0 && xx < g.n)
+      acc = fmaf(d, __bfloat162float(x[((static_cast<int64_t>(b) * g.H + yy + g.off) * g.W + xx + g.off) * g.C + c]),
+                 acc);
+    if (++xo == g.n) {   // next position (x fastest, then y, then the model)
+      xo = 0;
+      if (++yo == g.n) {
+        yo = 0;
+        ++b;
+      }
+    }
   }
   atomicAdd(dw + j, acc);
   if (j == 0) atomicAdd(db, accb);
@@ -654,6 +695,7 @@ int32_t ss_head_backward(const void* x, const int32_t* head, const float* w, con
   if (!x || !head || !w || !dpre || !dw || !db || !dpre_x) return fail(SS_ERR_INVALID, "bad arguments");
   const HeadGeom g{head[0], head[1], head[2], head[3], head[4], head[5]};
   if (9 * g.C > 1024) return fail(SS_ERR_UNSUPPORTED, "head with more than 113 channels");
+  if (static_cast<long long>(g.B) * g.n * g.n >= (1LL << 31)) return fail(SS_ERR_UNSUPPORTED, "head output beyond 2^31 values");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   head_wgrad_kernel<<<296, 9 * g.C, 0, st>>>(static_cast<const bf16*>(x), g, dpre, dw, db);
   const long long total = static_cast<long long>(g.B) * g.H * g.W * g.C;
