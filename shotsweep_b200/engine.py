@@ -121,6 +121,79 @@ class Engine:
                                           _lib.ptr(ws), ws.numel(), self._stream()), 'ss_gradient')
         return grad, illum
 
+    def images_from_host(self, vel, wavelet, obs_host, v_mute=None, t_mute=0.12, eps=1e-4, laplacian=True,
+                         chunk_rows=None):
+        """Images of host-resident observations with the copies overlapped (pinned host img, illum).
+
+        The rows are imaged in chunks: chunk k+1's gathers move to the device on a copy stream while chunk k
+        is imaged (two device buffers), and each chunk's images return to pinned host memory behind it, so
+        that an end-to-end call costs about the imaging time plus one chunk's copy.  obs_host: CPU tensor
+        [B, S, nt, nx] float32, pinned or not (pageable rows are staged through pinned buffers).
+        """
+        g = self.g
+        B = vel.shape[0]
+        shape = (B, g.n_shots, g.nt, g.nx)
+        if not isinstance(obs_host, torch.Tensor) or obs_host.device.type != 'cpu' or obs_host.dtype != torch.float32:
+            raise ValueError('obs_host must be a float32 CPU tensor')
+        if tuple(obs_host.shape) != shape:
+            raise ValueError(f'obs must have shape {shape}, got {tuple(obs_host.shape)}')
+        obs_host = obs_host.contiguous()
+        if chunk_rows:
+            chunk = int(chunk_rows)
+        else:   # about six chunks, each a whole number of rounds of the persistent clusters
+            slots = self.plan(B, _lib.MODE_IMAGES)['slots']
+            per_round = slots // math.gcd(slots, g.n_shots)          # rows whose solves fill whole rounds
+            chunk = max(1, min(B, math.ceil(math.ceil(B / 6) / per_round) * per_round))
+        n_chunks = math.ceil(B / chunk)
+        dev = self.device
+        compute = torch.cuda.current_stream(dev)
+        if getattr(self, '_copy_stream', None) is None:
+            self._copy_stream = torch.cuda.Stream(dev)
+        copy = self._copy_stream
+        f32 = dict(dtype=torch.float32, device=dev)
+        dev_obs = [torch.empty(chunk, *shape[1:], **f32) for _ in range(min(2, n_chunks))]
+        pinned = obs_host.is_pinned()
+        staging = [] if pinned else [torch.empty(chunk, *shape[1:], dtype=torch.float32, pin_memory=True)
+                                     for _ in range(min(2, n_chunks))]
+        img_dev = torch.empty(B, g.n_shots, g.nz, g.nx, **f32)
+        illum_dev = torch.empty_like(img_dev)
+        img = torch.empty(img_dev.shape, dtype=torch.float32, pin_memory=True)
+        illum = torch.empty_like(img, pin_memory=True)
+        flags = torch.zeros(n_chunks, dtype=torch.int32, device=dev)
+        copied = [torch.cuda.Event() for _ in dev_obs]
+        imaged = [torch.cuda.Event() for _ in dev_obs]
+        for k in range(n_chunks):
+            a, b = k * chunk, min(B, (k + 1) * chunk)
+            buf = k % len(dev_obs)
+            src = obs_host[a:b]
+            if not pinned:
+                if k >= len(staging):
+                    copied[buf].synchronize()          # the staging buffer's previous rows have left
+                staging[buf][:b - a].copy_(src)
+                src = staging[buf][:b - a]
+            with torch.cuda.stream(copy):
+                if k >= len(dev_obs):
+                    copy.wait_event(imaged[buf])       # the device buffer's previous chunk is imaged
+                dev_obs[buf][:b - a].copy_(src, non_blocking=True)
+                copied[buf].record(copy)
+            compute.wait_event(copied[buf])
+            self.images(vel[a:b], wavelet, dev_obs[buf][:b - a], None if v_mute is None else v_mute[a:b], t_mute, eps,
+                        laplacian, out=(img_dev[a:b], illum_dev[a:b]))
+            flags[k:k + 1].copy_(self._ws[:4].view(torch.int32))   # this chunk's device status, kept
+            imaged[buf].record(compute)
+            with torch.cuda.stream(copy):
+                copy.wait_event(imaged[buf])
+                img[a:b].copy_(img_dev[a:b], non_blocking=True)
+                illum[a:b].copy_(illum_dev[a:b], non_blocking=True)
+        copy.synchronize()
+        compute.synchronize()
+        bad = flags.cpu().numpy()
+        if (bad == _lib.ERR_NONFINITE).any():
+            raise ValueError('observations must be finite')
+        if bad.any():
+            _lib.check(int(bad[bad != 0][0]), 'device status')
+        return img, illum
+
     def images(self, vel, wavelet, obs, v_mute=None, t_mute=0.12, eps=1e-4, laplacian=True, want_grad=False,
                out=None):
         """(img, illum[, grad]), each [B, S, nz, nx]."""

@@ -136,7 +136,8 @@ class Sim:
     @staticmethod
     def _velocity(v):
         v = np.asarray(v, np.float64)
-        if v.ndim != 3 or v.shape[1:] != (NZ, NX) or not np.isfinite(v).all() or np.any(v <= 0):
+        t = torch.from_numpy(v)           # the checks on all host threads
+        if v.ndim != 3 or v.shape[1:] != (NZ, NX) or not bool(torch.isfinite(t).all()) or bool((t <= 0).any()):
             raise ValueError(f'velocities must be finite positive (B, {NZ}, {NX}) arrays')   # gpu.py:103-104
         return v
 
@@ -221,6 +222,18 @@ class Sim:
             raise ValueError('illumination regularization eps must be positive')
         v = self._velocity(v_bg)
         B = len(v)
+        host = not (isinstance(obs, torch.Tensor) and obs.is_cuda)
+        if host:   # host observations: copies overlapped with imaging, chunk by chunk
+            o = obs if isinstance(obs, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(obs))
+            o = o.to(torch.float32) if o.dtype != torch.float32 else o
+            if tuple(o.shape) != (B, 5, NT, NX):                                   # gpu.py:156-157
+                raise ValueError(f'observations must be finite with shape {(B, 5, NT, NX)}')
+            try:
+                img, illum = self.engine.images_from_host(self._to_dev(v), self._wavelet(), o, self._mute(v_mute, B),
+                                                          t_mute, eps, laplacian)
+            except ValueError:
+                raise ValueError(f'observations must be finite with shape {(B, 5, NT, NX)}') from None
+            return img.numpy(), illum.numpy()
         img, illum = self.engine.images(self._to_dev(v), self._wavelet(), self._observed(obs, B),
                                         self._mute(v_mute, B), t_mute, eps, laplacian)
         self._finish(B)
