@@ -215,12 +215,19 @@ template <int BN, int EPI>
 int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits, cudaStream_t st) {
   auto kern = gemm_bf16_kernel<BN, EPI>;
   constexpr size_t smem = gemm_smem_bytes<BN>();
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [&] {
-    attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  });
-  if (attr_err != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(attr_err));
+  // the attribute is per device: set once on each device that launches this instantiation
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  SS_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SS_ERR_UNSUPPORTED, "device index beyond 63");
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done[dev]) {
+      SS_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      done[dev] = true;
+    }
+  }
   dim3 grid((g.N + BN - 1) / BN, (g.M + kBM - 1) / kBM, splits);
   kern<<<grid, kGemmThreads, smem, st>>>(ta, tb, g);
   SS_TRY_CUDA(cudaGetLastError());
