@@ -2,6 +2,7 @@
 
     python -m shotsweep_b200.profiling [n_models]
     python -m shotsweep_b200.profiling learned [batch]
+    python -m shotsweep_b200.profiling uneven [solves]
 
 The second form: `batch` simulated models (default 64), three training steps of the learned
 proposal (warm-up), then five timed steps; each step launches the network's 38 tensor-core
@@ -73,8 +74,41 @@ def learned(batch=64):
     print(f'batch={batch} training step {e0.elapsed_time(e1) / 5:.3f} ms, L1 {net.loss_sum.item() / (batch * 4900):.4f}')
 
 
+def uneven(n_solves=48):
+    """A seeded uneven batch (time axes capped at 600 steps), forward then images twice (the second timed)."""
+    import dataclasses
+    from .batch import Shape, UnevenBatch
+    wl = synth.uneven_workload(n_solves, seed=9)
+    shapes, bgs, truths = [], [], []
+    for m in wl:
+        nz, nx = m['truth'].shape
+        for bg in m['backgrounds']:
+            shapes.append(Shape(nz, nx, min(m['nt'], 600), m['shot_cols'], v_mute=m['v_s']))
+            bgs.append(bg)
+            truths.append(m['truth'])
+    b = UnevenBatch(shapes)
+    dev = b.device
+    t = np.arange(b.max_nt) * 1e-3
+    a = (np.pi * 15.0 * (t - 1.2 / 15.0)) ** 2
+    w = torch.tensor((1 - 2 * a) * np.exp(-a) * 1e3, dtype=torch.float32, device=dev)
+    obs = b.forward(b.pack_models(truths), w)
+    vb = b.pack_models(bgs)
+    b.images(vb, w, obs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.images(vb, w, obs)
+    e1.record()
+    torch.cuda.synchronize()
+    b.status()
+    print(f'solves={b.n_solves} classes={[(c["cluster"], c["n_solves"]) for c in b.classes()]} '
+          f'images {e0.elapsed_time(e1):.3f} ms')
+
+
 if __name__ == '__main__':
     if len(sys.argv) > 1 and sys.argv[1] == 'learned':
         learned(int(sys.argv[2]) if len(sys.argv) > 2 else 64)
+    elif len(sys.argv) > 1 and sys.argv[1] == 'uneven':
+        uneven(int(sys.argv[2]) if len(sys.argv) > 2 else 48)
     else:
         main(int(sys.argv[1]) if len(sys.argv) > 1 else 9)
