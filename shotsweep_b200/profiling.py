@@ -3,6 +3,10 @@
     python -m shotsweep_b200.profiling [n_models]
     python -m shotsweep_b200.profiling learned [batch]
     python -m shotsweep_b200.profiling uneven [solves]
+    python -m shotsweep_b200.profiling gemm
+
+The last form times the tensor-core GEMM on square BF16 problems (4096^3, 8192^3; BF16 and F32 outputs)
+beside torch.matmul on the same device.
 
 The second form: `batch` simulated models (default 64), three training steps of the learned
 proposal (warm-up), then five timed steps; each step launches the network's 38 tensor-core
@@ -105,9 +109,44 @@ def uneven(n_solves=48):
           f'images {e0.elapsed_time(e1):.3f} ms')
 
 
+def gemm():
+    from . import _lib
+    L = _lib.load()
+    dev = torch.device('cuda', torch.cuda.current_device())
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 10
+
+    for n in (4096, 8192):
+        A = torch.randn(n, n, device=dev).to(torch.bfloat16)
+        B = torch.randn(n, n, device=dev).to(torch.bfloat16)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        for epi, dt in ((_lib.EPI_BIAS_LRELU_BF16, torch.bfloat16), (_lib.EPI_F32, torch.float32)):
+            C = torch.empty(n, n, dtype=dt, device=dev)
+            ms = timed(lambda: _lib.check(L.ss_gemm_bf16(_lib.ptr(A), n, _lib.ptr(B), n, n, n, n, epi, _lib.ptr(C), n,
+                                                         None, 1.0, 1, _lib.ptr(err), _lib.stream_handle(dev)),
+                                          'ss_gemm_bf16'))
+            print(f'n={n} ss_gemm_bf16 {"bf16" if epi == _lib.EPI_BIAS_LRELU_BF16 else "f32"} out: {ms:.3f} ms, '
+                  f'{2 * n ** 3 / ms / 1e9:.0f} TFLOP/s, status {err.item()}')
+        ref = torch.empty(n, n, dtype=torch.bfloat16, device=dev)
+        ms = timed(lambda: torch.matmul(A, B.T, out=ref))
+        print(f'n={n} torch.matmul bf16 out: {ms:.3f} ms, {2 * n ** 3 / ms / 1e9:.0f} TFLOP/s')
+
+
 if __name__ == '__main__':
     if len(sys.argv) > 1 and sys.argv[1] == 'learned':
         learned(int(sys.argv[2]) if len(sys.argv) > 2 else 64)
+    elif len(sys.argv) > 1 and sys.argv[1] == 'gemm':
+        gemm()
     elif len(sys.argv) > 1 and sys.argv[1] == 'uneven':
         uneven(int(sys.argv[2]) if len(sys.argv) > 2 else 48)
     else:
