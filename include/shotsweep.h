@@ -203,6 +203,13 @@ int32_t ss_images_noalloc(const ss_geometry* geom, int32_t n_models, const float
  * caller times the launch on `stream`; `out` must hold one float. */
 int32_t ss_fp32_probe(float* out, int32_t blocks, int32_t iters, int32_t packed, double* flops, void* stream);
 
+/* Failure-detection probe (no counterpart in the reference): one warp runs the
+ * simulation kernels' bounded mbarrier wait on a barrier that nothing arrives
+ * on; after limit_ms (0 < limit_ms <= 10000) it writes SS_ERR_TIMEOUT to
+ * *status (device int) and returns, as a stalled solve would, without hanging
+ * or faulting the GPU. */
+int32_t ss_wait_probe(int32_t* status, double limit_ms, void* stream);
+
 /* ---- Uneven batches ------------------------------------------------------
  * Models of different grid size, step count and shot count in one launch
  * sequence.  No counterpart in the reference, whose Sim is fixed to one

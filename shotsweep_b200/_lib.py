@@ -147,6 +147,7 @@ _SIGNATURES = {
                                       _P, _P]),
     'ss_lbfgs_push': (ctypes.c_int32, [_P, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
                                        ctypes.c_int32, _P]),
+    'ss_wait_probe': (ctypes.c_int32, [_P, ctypes.c_double, _P]),
     'ss_images_noalloc': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P]),
 }

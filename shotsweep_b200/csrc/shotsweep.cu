@@ -36,6 +36,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/shotsweep.h"
 #include "internal.h"
 
@@ -51,6 +53,12 @@ constexpr size_t kMaxSmem = 227 * 1024;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s per bounded wait
 
 thread_local std::string g_last_error;
+
+// NVTX range around an entry point (header-only NVTX: free unless a profiler is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -123,11 +131,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 // Bounded wait: gives up after kWaitLimitNs, records SS_ERR_TIMEOUT and
 // returns, so that every thread still reaches every barrier of the kernel.
-__device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity, int* err) {
+__device__ __forceinline__ void mbar_wait_bounded(uint32_t bar, uint32_t parity, int* err,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > kWaitLimitNs) {
+    if (global_ns() - t0 > limit_ns) {
       atomicExch(err, static_cast<int>(SS_ERR_TIMEOUT));
       return;
     }
@@ -574,6 +583,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       S.f[1] = solve_smem + field_floats;
       S.stg0 = solve_smem + 2 * field_floats;
       S.dummy = S.stg0 + kStages * stage_floats;
+      {   // self-check: this solve's part of shared memory must fit the launch's allocation
+        uint32_t dyn = 0;
+        asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+        const size_t end = reinterpret_cast<const unsigned char*>(S.dummy + (H + 4) * gs.rs + H * gs.sw) - smem_raw;
+        if (end > dyn || gs.nact > nthr) {
+          if (tid == 0) atomicExch(P.err, static_cast<int>(SS_ERR_UNSUPPORTED));
+          continue;   // uniform across the cluster: every CTA sees the same solve and sizes
+        }
+      }
     } else {
       if (it >= P.n_solves) break;
       solve = it;
@@ -1156,6 +1174,16 @@ __global__ void finish_kernel(KParams P, const float* __restrict__ gacc, const f
   }
 }
 
+// Failure-detection probe: the solve kernel's bounded mbarrier wait on a
+// barrier that nothing arrives on.  It must give up after `limit_ns`, record
+// SS_ERR_TIMEOUT and return, leaving the context usable.
+__global__ void wait_probe_kernel(int* status, unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(smem_u32(&bar), 1);
+  __syncthreads();
+  mbar_wait_bounded(smem_u32(&bar), 0u, status, limit_ns);
+}
+
 // FP32 throughput probe: 8 independent FMA chains per thread, scalar or
 // packed FP32x2, for the roofline denominator of the stencil kernels.
 template <bool PACKED>
@@ -1376,6 +1404,7 @@ int launch(const Plan& p, int mode, const KParams& k, cudaStream_t stream) {
 int run_adjoint(int mode, const ss_geometry* g, int n_models, const float* vel, const float* wavelet, const float* obs,
                 const float* v_mute, float t_mute, float eps, int laplacian, float* img, float* illum, float* grad,
                 void* ws, size_t ws_bytes, void* stream) {
+  NvtxRange range(mode == SS_MODE_IMAGES ? "ss_images" : "ss_gradient");
   g_last_error.clear();
   int rc = check_geometry(g);
   if (rc) return rc;
@@ -1809,6 +1838,7 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
 int batch_run(const void* plan, const void* plan_dev, const float* vel, const float* wavelet, const float* obs,
               float t_mute, float eps, int laplacian, float* gathers, float* img, float* illum, float* grad, void* ws,
               size_t ws_bytes, void* stream) {
+  NvtxRange range("ss_batch_run");
   if (!plan || !plan_dev) return fail(SS_ERR_INVALID, "plan and its device copy are required");
   BatchPlanHeader h;
   std::memcpy(&h, plan, sizeof(h));
@@ -1960,6 +1990,7 @@ int32_t ss_plan_info(const ss_geometry* geom, int32_t n_models, int32_t mode, in
 
 int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet, float* gathers,
                    float* ckpt, int32_t ckpt_interval, void* workspace, size_t workspace_bytes, void* stream) {
+  NvtxRange range("ss_forward");
   g_last_error.clear();
   int rc = check_geometry(geom);
   if (rc) return rc;
@@ -2173,6 +2204,15 @@ int32_t ss_gradient_finish(const ss_geometry* geom, int32_t n_models, const floa
   const long long total = static_cast<long long>(n_models) * geom->n_shots * geom->nz * geom->nx;
   finish_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(k, gacc, src_acc, illum_acc, grad,
                                                                               illum);
+  SS_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_wait_probe(int32_t* status, double limit_ms, void* stream) {
+  g_last_error.clear();
+  if (!status || !(limit_ms > 0.0) || limit_ms > 10000.0) return fail(SS_ERR_INVALID, "bad arguments");
+  wait_probe_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+      status, static_cast<unsigned long long>(limit_ms * 1e6));
   SS_CUDA(cudaGetLastError());
   return SS_OK;
 }
