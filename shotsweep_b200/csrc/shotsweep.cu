@@ -1,11 +1,12 @@
 // libshotsweep: B200 (sm_100a) kernels for ShotSweep's physics hot path.
 //
 // One velocity model x one shot is a "solve".  Each solve runs on a thread-block
-// cluster of C CTAs (C = 2 for the 150x150 padded OpenFWI grid); the padded grid
-// is cut into C horizontal bands, one per CTA, and each CTA keeps its band of
-// the two most recent wavefields in shared memory for the whole time loop.
-// Neighbouring bands exchange their two edge rows every step through
-// distributed shared memory (DSMEM); one cluster barrier per step orders it.
+// cluster of C CTAs (C = 3 for the 150x150 padded OpenFWI grid); the padded grid
+// is cut into C horizontal bands, one per CTA.  Each thread keeps a 5 x 4 tile
+// of both time levels in registers for the whole time loop; shared memory holds
+// the current level of the band for the neighbouring tiles' stencils.
+// Neighbouring bands push their two edge rows into each other's halo rows every
+// step through distributed shared memory (st.async counted on mbarriers).
 //
 // Arithmetic (reference: openfwi/physics/gpu.py)
 //   forward   p[t+1] = p[t-1] + kappa*(p[t]-p[t-1]) + sigma*S(p[t])  (+ source)
@@ -22,7 +23,7 @@
 // Instead of the reference's checkpoint-and-recompute (gpu.py:131,169-176) the
 // forward stores S(p[t]) of every step to a per-cluster history in HBM with
 // TMA bulk copies (cp.async.bulk) and the adjoint streams it back in reverse,
-// prefetching one step ahead.  This trades 2x4 bytes of HBM traffic per cell
+// prefetching two steps ahead.  This trades 2x4 bytes of HBM traffic per cell
 // and step for the 16 flops per cell and step that a recompute would cost.
 
 #include <cuda_runtime.h>
@@ -78,21 +79,6 @@ int fail(int code, const std::string& msg) {
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ uint32_t cluster_rank() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_id() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ uint32_t cluster_count() {
-  uint32_t r;
-  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
-  return r;
-}
 __device__ __forceinline__ void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
@@ -100,11 +86,6 @@ __device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
   uint32_t r;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
   return r;
-}
-__device__ __forceinline__ void st_cluster_v4(uint32_t addr, float4 v) {
-  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
-               "f"(v.w)
-               : "memory");
 }
 __device__ __forceinline__ void st_cluster_u32(uint32_t addr, int v) {
   asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
@@ -152,7 +133,6 @@ __device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t byt
                : "memory");
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 // At most kStages-2 newer history stores may still be reading shared memory.
 __device__ __forceinline__ void bulk_wait_read_lag() {
   static_assert(kStages == 3, "the immediate below is kStages - 2");
@@ -164,13 +144,6 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 __device__ __forceinline__ void fence_proxy_async_all() { asm volatile("fence.proxy.async;" ::: "memory"); }
 
-// 9-point stencil times 12*dx^2: 16*(near) - (far) - 60*centre.
-__device__ __forceinline__ float stencil(float zm2, float zm1, float c, float zp1, float zp2, float xm2, float xm1,
-                                         float xp1, float xp2) {
-  const float near_ = (zm1 + zp1) + (xm1 + xp1);
-  const float far_ = (zm2 + zp2) + (xm2 + xp2);
-  return fmaf(-60.f, c, fmaf(16.f, near_, -far_));
-}
 
 // Normalised depth into the absorbing layer (gpu.py:85-87).
 __device__ __forceinline__ double layer_depth(int i, int n, int pad) {
@@ -385,21 +358,6 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
       : "memory");
 }
 
-__device__ __forceinline__ void st_async_v4(uint32_t addr, float4 v, uint32_t bar) {
-  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(addr),
-               "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(bar)
-               : "memory");
-}
-
-__device__ __forceinline__ float pick(const float4& v, int m) {
-  return m == 0 ? v.x : m == 1 ? v.y : m == 2 ? v.z : v.w;
-}
-__device__ __forceinline__ void add_at(float4& v, int m, float a) {
-  if (m == 0) v.x += a;
-  else if (m == 1) v.y += a;
-  else if (m == 2) v.z += a;
-  else v.w += a;
-}
 
 // Body of one tile row k (a compile-time constant after unrolling) inside
 // solve_kernel's step; written once, expanded in two row orders.
