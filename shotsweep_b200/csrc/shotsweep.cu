@@ -47,7 +47,8 @@ namespace {
 constexpr int kRowsPerThread = 5;          // H: rows per thread in the band
 constexpr int kMaxThreads = 384;           // register budget: 168 regs/thread
 constexpr int kMaxCluster = 16;
-constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush
+constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush (at most)
+constexpr int kMinTraceRing = 8;           // the fewest, for grids whose shared memory is tight
 constexpr int kStages = 3;                 // history slabs in flight: prefetch / retire depth kStages-1
 constexpr int kFastRS = 156;               // shared row stride of the 150-column padded OpenFWI grid
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -181,6 +182,7 @@ struct KParams {
   float dx, dt;
   int ncg, nseg, bh, C, rs, sw, nact;
   int nxs;         // trace row stride of the per-slot scratch (nx rounded up to 4)
+  int ring;        // receiver rows staged in shared memory per flush (a power of two, 8..32)
   int n_solves;
   const float* vel;
   const float* wav;
@@ -220,7 +222,7 @@ struct Smem {
   float* wav;
   float* red;
   float* res0;     // kStages residual rows of nxs, consecutive
-  float* trc;      // ring of kTraceRing receiver rows, flushed to global memory
+  float* trc;      // ring of P.ring receiver rows, flushed to global memory
   float* dummy;    // zero tile for lanes without cells: (H + 4) rows of RS, then H rows of sw
   uint64_t* bar;
 };
@@ -476,7 +478,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     S.red = S.wav + ((P.nt + 31) & ~31);
     S.res0 = S.red + 32;
     S.trc = S.res0 + kStages * NXS;
-    S.dummy = S.trc + kTraceRing * NXS;
+    S.dummy = S.trc + P.ring * NXS;
     S.bar = reinterpret_cast<uint64_t*>(S.dummy + (H + 4) * RS + H * SW);   // [0,kStages) history, then 2 halos
   } else {
     S.bar = reinterpret_cast<uint64_t*>(smem_raw);
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     S.red = S.wav + ((P.nt + 31) & ~31);
     S.res0 = S.red + 32;
     S.trc = S.res0 + kStages * NXS;
-    solve_smem = S.trc + kTraceRing * NXS;
+    solve_smem = S.trc + P.ring * NXS;
   }
   for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
   if (tid == 0) {
@@ -731,7 +733,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         // the previous step is now the read-only field X
         #pragma unroll 1
         for (int r = tid; r < NX; r += nthr)
-          S.trc[((lvl - 1) % kTraceRing) * NXS + r] = X[(src_r - row0 + 2) * RS + PAD + r + 2];
+          S.trc[((lvl - 1) & (P.ring - 1)) * NXS + r] = X[(src_r - row0 + 2) * RS + PAD + r + 2];
       }
       {
         // Lanes without a tile run the same code on a private zero tile
@@ -779,16 +781,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           #pragma unroll 1
           for (int i = tid; i < n; i += nthr) {
             const int tt = flushed + i / NX, r = i % NX;
-            trace[static_cast<size_t>(tt) * tstride + r] = S.trc[(tt % kTraceRing) * NXS + r];
+            trace[static_cast<size_t>(tt) * tstride + r] = S.trc[(tt & (P.ring - 1)) * NXS + r];
           }
           __syncthreads();
           flushed = hi + 1;
         };
-        if (lvl - flushed == kTraceRing) flush(lvl - 1);
+        if (lvl - flushed == P.ring) flush(lvl - 1);
         if (lvl == GNT - 1) {   // the last level, recorded after the final barrier
           #pragma unroll 1
         for (int r = tid; r < NX; r += nthr)
-            S.trc[(lvl % kTraceRing) * NXS + r] = Y[(src_r - row0 + 2) * RS + PAD + r + 2];
+            S.trc[(lvl & (P.ring - 1)) * NXS + r] = Y[(src_r - row0 + 2) * RS + PAD + r + 2];
           flush(lvl);
         }
       }
@@ -1171,7 +1173,7 @@ __global__ void __launch_bounds__(256) fp32_probe_kernel(float* out, int iters) 
 // Host side: plans, workspace, launches
 // ----------------------------------------------------------------------------
 struct Plan {
-  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads;
+  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads, ring;
   bool fast;
   size_t smem;
   int max_clusters;
@@ -1219,10 +1221,10 @@ SolveFn batch_kernel_for(int mode) {
   }
 }
 
-size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj) {
+size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring) {
   const size_t field = static_cast<size_t>(bh + 4) * rs;
   const size_t stage = adj ? static_cast<size_t>(bh) * sw : 0;
-  return (2 * field + kStages * stage + ((nt + 31) & ~31) + 32 + (kStages + kTraceRing) * static_cast<size_t>(nxs) +
+  return (2 * field + kStages * stage + ((nt + 31) & ~31) + 32 + (kStages + ring) * static_cast<size_t>(nxs) +
           (kRowsPerThread + 4) * static_cast<size_t>(rs) + kRowsPerThread * static_cast<size_t>(sw)) *
              sizeof(float) +
          (kStages + 2) * sizeof(uint64_t);
@@ -1245,15 +1247,19 @@ int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
     if (C > 1 && nseg < 1) break;
     const int bh = nseg * H;
     if (C > 1 && bh < 2) continue;
-    const size_t sm = smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj);
-    if (sm <= kMaxSmem) {
-      p->C = C;
-      p->nseg = nseg;
-      p->bh = bh;
-      p->smem = sm;
-      ok = true;
-      break;
+    // the deepest receiver ring that fits (wide grids with long time axes get a shallower one)
+    for (int ring = kTraceRing; ring >= kMinTraceRing && !ok; ring /= 2) {
+      const size_t sm = smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj, ring);
+      if (sm <= kMaxSmem) {
+        p->C = C;
+        p->nseg = nseg;
+        p->bh = bh;
+        p->smem = sm;
+        p->ring = ring;
+        ok = true;
+      }
     }
+    if (ok) break;
   }
   if (!ok) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits shared memory for this grid");
   p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
@@ -1336,6 +1342,7 @@ KParams base_params(const ss_geometry* g, const Plan& p, int n_models) {
   k.sw = p.sw;
   k.nact = p.ncg * p.nseg;
   k.nxs = (g->nx + 3) & ~3;
+  k.ring = p.ring > 0 ? p.ring : kTraceRing;
   k.n_solves = n_models * g->n_shots;
   k.hist_steps = g->nt;
   return k;
@@ -1443,10 +1450,10 @@ int noalloc_scratch(void** out) {
 // A plan is one contiguous blob, identical in host and device memory:
 // BatchPlanHeader, then BatchItemDev[n_items], then int order[n_solves]
 // (per class, solves longest-first).  The header carries the launch shapes.
-constexpr uint64_t kPlanMagic = 0x3130504853535342ull;   // "BSSSHP01"
+constexpr uint64_t kPlanMagic = 0x3230504853535342ull;   // "BSSSHP02"
 
 struct BatchClassHost {
-  int C, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter;
+  int C, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter, ring;
   int max_clusters, idle_sms;   // co-resident clusters alone on the GPU, and the SMs they leave idle
   size_t hist_slot, trace_slot, gpad_slot, grad_slot;   // floats per slot
   size_t ws_off;                                        // bytes: this class's scratch in the workspace
@@ -1464,8 +1471,8 @@ struct BatchPlanHeader {
 // Shared memory of a batch launch: the fixed part (barriers, wavelet,
 // reduction words, residual rows, receiver ring) and one solve's part
 // (two fields, the history slabs, the zero tile).
-size_t batch_fixed_smem(int nt_max, int nxs) {
-  return (16 + static_cast<size_t>((nt_max + 31) & ~31) + 32 + static_cast<size_t>(kStages + kTraceRing) * nxs) *
+size_t batch_fixed_smem(int nt_max, int nxs, int ring = kMinTraceRing) {
+  return (16 + static_cast<size_t>((nt_max + 31) & ~31) + 32 + static_cast<size_t>(kStages + ring) * nxs) *
          sizeof(float);
 }
 size_t batch_solve_smem(int bh, int ncg, bool adj) {
@@ -1676,7 +1683,13 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
     }
     k.trace_slot = static_cast<size_t>(k.nt_max) * k.nxs;
     k.threads = ((max_nact + 31) / 32) * 32;
-    k.smem = static_cast<int>(batch_fixed_smem(k.nt_max, k.nxs) + solve_part);
+    k.ring = kMinTraceRing;   // the deepest receiver ring that fits beside the class's largest solve
+    for (int ring = kTraceRing; ring > kMinTraceRing; ring /= 2)
+      if (batch_fixed_smem(k.nt_max, k.nxs, ring) + solve_part <= kMaxSmem) {
+        k.ring = ring;
+        break;
+      }
+    k.smem = static_cast<int>(batch_fixed_smem(k.nt_max, k.nxs, k.ring) + solve_part);
     // solves longest-first
     const int begin = static_cast<int>(order.size());
     for (int i : cls[c].items)
@@ -1835,6 +1848,7 @@ int batch_run(const void* plan, const void* plan_dev, const float* vel, const fl
     p.C = k.C;
     p.nt = k.nt_max;
     p.nxs = k.nxs;
+    p.ring = k.ring;
     p.bh = k.bh_max;
     p.n_solves = k.n_solves;
     p.items = reinterpret_cast<const BatchItemDev*>(pd + h.items_off);

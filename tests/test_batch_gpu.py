@@ -157,3 +157,28 @@ def test_batch_rejects_bad_input(case):
         b.images(case['vb'], case['wav'][:10].contiguous(), case['obs'])
     with pytest.raises(ValueError, match='vel'):
         b.images(case['vb'][:-1].contiguous(), case['wav'], case['obs'])
+
+
+def test_full_size_models_equal_single_geometry():
+    """The largest grids and time axes of the uneven workload (200 x 300 cells over 3000 steps, 150 x 250 over
+    2000): clusters of 14 and 9 CTAs in one batch, bit-identical to the single-geometry path."""
+    from oracle import oracle as O
+    from shotsweep_b200.batch import Shape, UnevenBatch, shot_columns
+    shs = [Shape(200, 300, 3000, shot_columns(300, 2), v_mute=1900.0), Shape(150, 250, 2000, shot_columns(250, 3))]
+    b = UnevenBatch(shs)
+    assert sorted(c['cluster'] for c in b.classes()) == sorted(c['min_cluster'] for c in b.classes())
+    assert max(c['cluster'] for c in b.classes()) >= 12
+    wav = torch.tensor(O.ricker(b.max_nt) * 1e3, dtype=torch.float32, device=b.device)
+    truths = models_for(shs, 8)
+    bgs = backgrounds_for(truths)
+    obs = b.forward(b.pack_models(truths), wav)
+    img, illum, _ = b.images(b.pack_models(bgs), wav, obs, t_mute=0.1)
+    b.status()
+    for i, sh in enumerate(shs):
+        eng = engine_for(sh)
+        vm = torch.tensor([sh.v_mute], device=b.device) if sh.v_mute > 0 else None
+        ref_img, ref_illum = eng.images(torch.tensor(bgs[i][None], device=b.device), wav[:sh.nt].contiguous(),
+                                        b.unpack_traces(obs, i)[None].contiguous(), vm, 0.1)
+        eng.status()
+        assert torch.equal(b.unpack_images(img, i), ref_img[0]), i
+        assert torch.equal(b.unpack_images(illum, i), ref_illum[0]), i
