@@ -362,8 +362,9 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
 
 
 // Body of one tile row k (a compile-time constant after unrolling) inside
-// solve_kernel's step; written once, expanded in two row orders.
-#define SS_TILE_ROW(k) \
+// solve_kernel's step; written once, expanded in two row orders, each with
+// (SPECIAL) and without the source / receiver terms.
+#define SS_TILE_ROW(k, SPECIAL) \
           const float4 rm2 = k >= 2 ? as4(O1[k - 2]) : (k == 0 ? h0 : h1); \
           const float4 rm1 = k >= 1 ? as4(O1[k - 1]) : h1; \
           const float4 rc = as4(O1[k]); \
@@ -377,7 +378,7 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
           const float2 n_hi = leapfrog(kap[k][1], nsig[k][1], O1[k][1], O2[k][1], s_hi); \
           float4 nw = make_float4(n_lo.x, n_lo.y, n_hi.x, n_hi.y); \
           if (fwd) { \
-            if (warp_src) {  /* injection after damping (gpu.py:113-114) */ \
+            if (SPECIAL) {  /* injection after damping (gpu.py:113-114) */ \
               const float a = (k == src_k) ? wt : 0.f; \
               nw.x += (src_m == 0) ? a : 0.f; \
               nw.y += (src_m == 1) ? a : 0.f; \
@@ -385,7 +386,7 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
               nw.w += (src_m == 3) ? a : 0.f; \
             } \
           } else { \
-            if (warp_rec) {  /* residual injection th += sigma*res (gpu.py:180) */ \
+            if (SPECIAL) {  /* residual injection th += sigma*res (gpu.py:180) */ \
               const float* rs = res_buf(bi); \
               const int rr = col0 - PAD; \
               const bool on = k == rec_k; \
@@ -396,7 +397,7 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
               nw.z = fmaf((on && rr + 2 >= 0 && rr + 2 < NX) ? -nsig[k][1].x : 0.f, r2v, nw.z); \
               nw.w = fmaf((on && rr + 3 >= 0 && rr + 3 < NX) ? -nsig[k][1].y : 0.f, r3v, nw.w); \
             } \
-            if (warp_src) {  /* source-strength term (gpu.py:182) */ \
+            if (SPECIAL) {  /* source-strength term (gpu.py:182) */ \
               const float a = (k == src_k) ? wt : 0.f; \
               const float q = src_m == 0 ? nw.x : src_m == 1 ? nw.y : src_m == 2 ? nw.z : nw.w; \
               src_acc = fmaf(q, a, src_acc); \
@@ -653,11 +654,11 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       src_k = src_r - myrow;
       src_m = src_c - col0;
     }
-    // rows of this thread with extra work: source, receivers, halo pushes
-    // Halo rows pushed inside the row loop.  Injections and the source term
-    // run behind warp-uniform branches: only warps holding such cells pay.
-    const bool warp_src = __any_sync(0xffffffffu, src_k >= 0);
-    const bool warp_rec = __any_sync(0xffffffffu, rec_k >= 0);
+    // Halo rows are pushed inside the row loop.  Injections and the source
+    // term are needed only by warps that hold a receiver (or source) cell:
+    // the step branches once on this warp-uniform flag into a row loop with
+    // that work and one without it, instead of testing it on every row.
+    const bool warp_special = __any_sync(0xffffffffu, src_k >= 0 || rec_k >= 0);
     const double v_src = v[(src_r - PAD) * NX + shot_col];
     const float amp = static_cast<float>((v_src / P.amp_ref) * (v_src / P.amp_ref));
 
@@ -750,17 +751,34 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         const float* hl = fwd ? nullptr : (active ? stage_buf(bi) + lr0 * SW + 4 * cg : dstg);
         auto as4 = [](const float2(&r)[2]) { return make_float4(r[0].x, r[0].y, r[1].x, r[1].y); };
         // Threads on the lower band edge compute their bottom rows first, so
-        // that the halo push to the next band leaves early in the step.
-        if (rev_rows) {
+        // that the halo push to the next band leaves early in the step.  The
+        // source and receiver terms are compiled into the rows of the first
+        // branch only (one warp-uniform branch per step instead of one per row).
+        if (warp_special) {
+          if (rev_rows) {
 #pragma unroll
-          for (int i = 0; i < H; ++i) {
-            const int k = H - 1 - i;
-            SS_TILE_ROW(k)
+            for (int i = 0; i < H; ++i) {
+              const int k = H - 1 - i;
+              SS_TILE_ROW(k, true)
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < H; ++k) {
+              SS_TILE_ROW(k, true)
+            }
           }
         } else {
+          if (rev_rows) {
 #pragma unroll
-          for (int k = 0; k < H; ++k) {
-            SS_TILE_ROW(k)
+            for (int i = 0; i < H; ++i) {
+              const int k = H - 1 - i;
+              SS_TILE_ROW(k, false)
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < H; ++k) {
+              SS_TILE_ROW(k, false)
+            }
           }
         }
       }
