@@ -125,10 +125,14 @@ class Engine:
                          chunk_rows=None):
         """Images of host-resident observations with the copies overlapped (pinned host img, illum).
 
-        The rows are imaged in chunks: chunk k+1's gathers move to the device on a copy stream while chunk k
-        is imaged (two device buffers), and each chunk's images return to pinned host memory behind it, so
-        that an end-to-end call costs about the imaging time plus one chunk's copy.  obs_host: CPU tensor
+        The rows are imaged in chunks.  Gathers (and, for host velocities, the model rows) move to the
+        device on one copy stream, at most two chunks ahead of the imaging (two device buffers); images
+        return to pinned host memory on a second copy stream behind each chunk.  The chunks grow from one
+        round of the persistent clusters, so that imaging starts after a short first copy, and the last one
+        is small, so that little is left to copy back at the end: a call costs about the imaging time.
+        vel: [B, nz, nx] float32, on the device or on the host (pinned or not).  obs_host: CPU tensor
         [B, S, nt, nx] float32, pinned or not (pageable rows are staged through pinned buffers).
+        `chunk_rows` fixes a uniform chunk size instead.
         """
         g = self.g
         B = vel.shape[0]
@@ -138,19 +142,24 @@ class Engine:
         if tuple(obs_host.shape) != shape:
             raise ValueError(f'obs must have shape {shape}, got {tuple(obs_host.shape)}')
         obs_host = obs_host.contiguous()
-        if chunk_rows:
-            chunk = int(chunk_rows)
-        else:   # about six chunks, each a whole number of rounds of the persistent clusters
-            slots = self.plan(B, _lib.MODE_IMAGES)['slots']
-            per_round = slots // math.gcd(slots, g.n_shots)          # rows whose solves fill whole rounds
-            chunk = max(1, min(B, math.ceil(math.ceil(B / 6) / per_round) * per_round))
-        n_chunks = math.ceil(B / chunk)
         dev = self.device
-        compute = torch.cuda.current_stream(dev)
-        if getattr(self, '_copy_stream', None) is None:
-            self._copy_stream = torch.cuda.Stream(dev)
-        copy = self._copy_stream
         f32 = dict(dtype=torch.float32, device=dev)
+        host_vel = isinstance(vel, torch.Tensor) and vel.device.type == 'cpu'
+        if host_vel:
+            if vel.dtype != torch.float32 or tuple(vel.shape) != (B, g.nz, g.nx):
+                raise ValueError(f'vel must be a float32 tensor of shape {(B, g.nz, g.nx)}')
+            vel_host = vel.contiguous() if vel.is_pinned() else vel.contiguous().pin_memory()
+            vel = torch.empty(B, g.nz, g.nx, **f32)
+        else:
+            vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
+        bounds = self._chunks(B, chunk_rows)
+        n_chunks = len(bounds)
+        chunk = max(b - a for a, b in bounds)
+        compute = torch.cuda.current_stream(dev)
+        if getattr(self, '_copy_streams', None) is None:
+            self._copy_streams = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+        h2d, d2h = self._copy_streams
+        h2d.wait_stream(compute)          # inputs and outputs made on the caller's stream are ready
         dev_obs = [torch.empty(chunk, *shape[1:], **f32) for _ in range(min(2, n_chunks))]
         pinned = obs_host.is_pinned()
         staging = [] if pinned else [torch.empty(chunk, *shape[1:], dtype=torch.float32, pin_memory=True)
@@ -162,8 +171,7 @@ class Engine:
         flags = torch.zeros(n_chunks, dtype=torch.int32, device=dev)
         copied = [torch.cuda.Event() for _ in dev_obs]
         imaged = [torch.cuda.Event() for _ in dev_obs]
-        for k in range(n_chunks):
-            a, b = k * chunk, min(B, (k + 1) * chunk)
+        for k, (a, b) in enumerate(bounds):
             buf = k % len(dev_obs)
             src = obs_host[a:b]
             if not pinned:
@@ -171,21 +179,24 @@ class Engine:
                     copied[buf].synchronize()          # the staging buffer's previous rows have left
                 staging[buf][:b - a].copy_(src)
                 src = staging[buf][:b - a]
-            with torch.cuda.stream(copy):
+            with torch.cuda.stream(h2d):
                 if k >= len(dev_obs):
-                    copy.wait_event(imaged[buf])       # the device buffer's previous chunk is imaged
+                    h2d.wait_event(imaged[buf])        # the device buffer's previous chunk is imaged
                 dev_obs[buf][:b - a].copy_(src, non_blocking=True)
-                copied[buf].record(copy)
+                if host_vel:
+                    vel[a:b].copy_(vel_host[a:b], non_blocking=True)
+                copied[buf].record(h2d)
             compute.wait_event(copied[buf])
             self.images(vel[a:b], wavelet, dev_obs[buf][:b - a], None if v_mute is None else v_mute[a:b], t_mute, eps,
                         laplacian, out=(img_dev[a:b], illum_dev[a:b]))
             flags[k:k + 1].copy_(self._ws[:4].view(torch.int32))   # this chunk's device status, kept
             imaged[buf].record(compute)
-            with torch.cuda.stream(copy):
-                copy.wait_event(imaged[buf])
+            with torch.cuda.stream(d2h):
+                d2h.wait_event(imaged[buf])
                 img[a:b].copy_(img_dev[a:b], non_blocking=True)
                 illum[a:b].copy_(illum_dev[a:b], non_blocking=True)
-        copy.synchronize()
+        h2d.synchronize()
+        d2h.synchronize()
         compute.synchronize()
         bad = flags.cpu().numpy()
         if (bad == _lib.ERR_NONFINITE).any():
@@ -193,6 +204,27 @@ class Engine:
         if bad.any():
             _lib.check(int(bad[bad != 0][0]), 'device status')
         return img, illum
+
+    def _chunks(self, B, chunk_rows=None):
+        """Row ranges [(a, b), ...] of the host-observation pipeline.
+
+        Default: whole rounds of the persistent clusters (rows whose solves fill every cluster), growing
+        from one round by x6 per chunk (a chunk's gathers cross PCIe several times faster than the previous
+        chunk is imaged) up to a third of the rows or 1 GiB of gathers; the last chunk takes what is left.
+        """
+        if chunk_rows:
+            c = int(chunk_rows)
+            return [(a, min(B, a + c)) for a in range(0, B, c)]
+        slots = self.plan(B, _lib.MODE_IMAGES)['slots']
+        per_round = slots // math.gcd(slots, self.g.n_shots)
+        row_bytes = self.g.n_shots * self.g.nt * self.g.nx * 4
+        cap = max(1, min(math.ceil(math.ceil(B / per_round) / 3), (1 << 30) // (row_bytes * per_round)))
+        out, a, n = [], 0, 1
+        while a < B:
+            b = min(B, a + min(n, cap) * per_round)
+            out.append((a, b))
+            a, n = b, n * 6
+        return out
 
     def images(self, vel, wavelet, obs, v_mute=None, t_mute=0.12, eps=1e-4, laplacian=True, want_grad=False,
                out=None):

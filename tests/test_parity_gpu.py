@@ -131,6 +131,26 @@ def test_batch_larger_than_resident_clusters_is_deterministic(gpu):
         np.testing.assert_array_equal(illum1[0], illum[i])
 
 
+def test_host_pipeline_equals_device_images(gpu):
+    """The chunked host-observation pipeline (device or host velocities, pinned or pageable gathers, uniform
+    or growing chunks) gives the device-resident images bit for bit."""
+    from shotsweep_b200 import engine, synth
+    sim = gpu.Sim()
+    eng = sim.engine
+    models = synth.population(30)
+    obs = torch.tensor(sim.gathers(models))
+    bgs = torch.tensor(np.stack([np.tile(np.linspace(1600, 3800, 70)[:, None], (1, 70)) + 7 * i
+                                 for i in range(30)]), dtype=torch.float32)
+    vm = torch.full((30,), 1800.0, device=eng.device)
+    w = engine.scaled_wavelet(gpu.RICKER, eng.device)
+    ref_img, ref_illum = eng.images(bgs.to(eng.device), w, obs.to(eng.device), vm, 0.12)
+    eng.status()
+    assert [b - a for a, b in eng._chunks(30)][:2] == [9, 18]
+    for vel, o, rows in ((bgs, obs.pin_memory(), None), (bgs.to(eng.device), obs, 7), (bgs.pin_memory(), obs, None)):
+        img, illum = eng.images_from_host(vel, w, o, vm, 0.12, chunk_rows=rows)
+        assert torch.equal(img, ref_img.cpu()) and torch.equal(illum, ref_illum.cpu())
+
+
 ODD = [
     # nz, nx, nt, pad, shot columns, src_row
     (23, 37, 160, 9, (0, 18, 36), 1),
