@@ -128,6 +128,19 @@ int32_t ss_images(const ss_geometry* geom, int32_t n_models, const float* vel, c
                   float* img, float* illum, float* grad,
                   void* workspace, size_t workspace_bytes, void* stream);
 
+/* Forward modelling and gradient with one source wavelet per velocity model.
+ * The reference's multiscale FWI estimates a wavelet for each model and
+ * frequency band (archive/toy/slopes/fwi.py:85-90, 144-146) and runs its
+ * forward and gradient with it (fwi.py:46-77); these run a whole batch of
+ * models, each with its own wavelet, in one launch.
+ *   wavelets [n_models, nt]   scaled source samples of each model
+ * Everything else as ss_forward (without checkpoints) and ss_gradient. */
+int32_t ss_forward_wavelets(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelets,
+                            float* gathers, void* workspace, size_t workspace_bytes, void* stream);
+int32_t ss_gradient_wavelets(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelets,
+                             const float* obs, const float* v_mute, float t_mute, float* grad, float* illum,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
 /* Checkpointed adjoint for differentiation (torch.autograd): the forward
  * keeps only the states (p[t-1], p[t]) every K = ckpt_interval steps
  * (ss_forward with ckpt), and the gradient is rebuilt segment by segment,

@@ -98,3 +98,40 @@ def fwi(sim, obs, v0, iters, smooth=2.0, mem=6, cap=50.0, c=1e-4, halvings=6, lo
         v, J, g = vt, Jt, gn
         history.append(J)
     return v, history
+
+
+def lowpass(x, fc, axis=1, dt=1e-3):
+    """fwi.py:78-83: Gaussian low-pass exp(-0.5 (f/fc)^4) along `axis`; fc None leaves x unchanged."""
+    if fc is None:
+        return x
+    n = x.shape[axis]
+    f = np.fft.rfftfreq(n, dt)
+    h = np.exp(-0.5 * (f / fc) ** 4)
+    shape = [1] * x.ndim
+    shape[axis] = len(f)
+    return np.fft.irfft(np.fft.rfft(x, axis=axis) * h.reshape(shape), n=n, axis=axis)
+
+
+def estimate_source(sim, obs, ricker, eps=1e-3):
+    """fwi.py:85-90 for one model's gathers [shots, nt, nx]: the Ricker shaped by the pooled Wiener filter."""
+    sf = np.fft.rfft(sim, axis=1)
+    of = np.fft.rfft(obs, axis=1)
+    num = (np.conj(sf) * of).sum(axis=(0, 2))
+    den = (np.abs(sf) ** 2).sum(axis=(0, 2))
+    shaping = num / (den + eps * den.max())
+    return np.fft.irfft(np.fft.rfft(ricker) * shaping, n=len(ricker))
+
+
+def fwi_bands(make_sim, obs, v0, ricker, bands=(8.0, None), iters=(10, 25), **kw):
+    """fwi.py:144-163 for one model: per band, low-passed gathers and Ricker, a Wiener-estimated wavelet,
+    then the L-BFGS loop with a fresh history.  make_sim(wavelet) -> OracleSim injecting that (unscaled)
+    wavelet.  Returns (v, [(band, wavelet, [J per iteration])])."""
+    v = np.asarray(v0, np.float64).copy()
+    out = []
+    for k, (fc, nit) in enumerate(zip(bands, iters)):
+        obs_b = lowpass(np.asarray(obs, np.float64), fc)
+        ric = lowpass(np.asarray(ricker, np.float64)[None, :, None], fc)[0, :, 0]
+        wav = estimate_source(make_sim(ric).gathers(v[None])[0].astype(np.float64), obs_b, ric)
+        v, hist = fwi(make_sim(wav), obs_b, v, nit, **kw)
+        out.append((k, wav, hist))
+    return v, out

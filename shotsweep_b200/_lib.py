@@ -88,6 +88,10 @@ _SIGNATURES = {
                                      _P, _P, _P, ctypes.c_size_t, _P]),
     'ss_images': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float,
                                    ctypes.c_float, ctypes.c_int32, _P, _P, _P, _P, ctypes.c_size_t, _P]),
+    'ss_forward_wavelets': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P,
+                                             ctypes.c_size_t, _P]),
+    'ss_gradient_wavelets': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, _P, _P, _P, _P,
+                                              ctypes.c_float, _P, _P, _P, ctypes.c_size_t, _P]),
     'ss_lap_f32': (ctypes.c_int32, [_P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P]),
     'ss_lap_f64': (ctypes.c_int32, [_P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P]),
     'ss_lap_adjoint_f32': (ctypes.c_int32, [_P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P]),

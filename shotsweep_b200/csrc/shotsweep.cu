@@ -186,6 +186,7 @@ struct KParams {
   int n_solves;
   const float* vel;
   const float* wav;
+  long long wav_stride;   // floats between consecutive models' wavelets; 0: one wavelet for all
   const float* obs;
   const float* vmute;
   float t_mute;
@@ -667,7 +668,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     int flushed = 0;       // receiver rows below this level are in global memory
     float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + trc_off : P.trace + static_cast<size_t>(slot) * trace_slot;
 
-    // ---- zero both shared fields (own rows and halos) --------------------
+    // ---- this model's wavelet (one per model: forward and gradient modes),
+    // both shared fields zeroed.  Every thread has passed the previous
+    // solve's last step barrier, after which nothing reads the staged
+    // wavelet; the cluster barrier below orders the new samples before the
+    // first step.
+    if ((MODE == SS_MODE_FORWARD || MODE == SS_MODE_GRADIENT) && !BATCH && P.wav_stride) {
+      const float* wm = P.wav + static_cast<size_t>(b) * P.wav_stride;
+      for (int i = tid; i < P.nt; i += nthr) S.wav[i] = wm[i];
+    }
     for (size_t i = tid; i < field_floats / 2; i += nthr) {
       reinterpret_cast<float2*>(S.f[0])[i] = make_float2(0.f, 0.f);
       reinterpret_cast<float2*>(S.f[1])[i] = make_float2(0.f, 0.f);
@@ -1386,7 +1395,7 @@ int launch(const Plan& p, int mode, const KParams& k, cudaStream_t stream) {
 
 int run_adjoint(int mode, const ss_geometry* g, int n_models, const float* vel, const float* wavelet, const float* obs,
                 const float* v_mute, float t_mute, float eps, int laplacian, float* img, float* illum, float* grad,
-                void* ws, size_t ws_bytes, void* stream) {
+                void* ws, size_t ws_bytes, void* stream, long long wav_stride = 0) {
   NvtxRange range(mode == SS_MODE_IMAGES ? "ss_images" : "ss_gradient");
   g_last_error.clear();
   int rc = check_geometry(g);
@@ -1407,6 +1416,7 @@ int run_adjoint(int mode, const ss_geometry* g, int n_models, const float* vel, 
   KParams k = base_params(g, p, n_models);
   k.vel = vel;
   k.wav = wavelet;
+  k.wav_stride = wav_stride;
   k.obs = obs;
   k.vmute = v_mute;
   k.t_mute = t_mute;
@@ -1978,8 +1988,9 @@ int32_t ss_plan_info(const ss_geometry* geom, int32_t n_models, int32_t mode, in
   return SS_OK;
 }
 
-int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet, float* gathers,
-                   float* ckpt, int32_t ckpt_interval, void* workspace, size_t workspace_bytes, void* stream) {
+static int run_forward(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
+                       float* gathers, float* ckpt, int32_t ckpt_interval, void* workspace, size_t workspace_bytes,
+                       void* stream, long long wav_stride) {
   NvtxRange range("ss_forward");
   g_last_error.clear();
   int rc = check_geometry(geom);
@@ -1997,6 +2008,7 @@ int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, 
   KParams k = base_params(geom, p, n_models);
   k.vel = vel;
   k.wav = wavelet;
+  k.wav_stride = wav_stride;
   k.gathers = gathers;
   k.ckpt = ckpt;
   k.ckpt_interval = ckpt ? ckpt_interval : 1;
@@ -2005,11 +2017,30 @@ int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, 
   return launch(p, SS_MODE_FORWARD, k, st);
 }
 
+int32_t ss_forward(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet, float* gathers,
+                   float* ckpt, int32_t ckpt_interval, void* workspace, size_t workspace_bytes, void* stream) {
+  return run_forward(geom, n_models, vel, wavelet, gathers, ckpt, ckpt_interval, workspace, workspace_bytes, stream, 0);
+}
+
+int32_t ss_forward_wavelets(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelets,
+                            float* gathers, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!geom) return check_geometry(geom);
+  return run_forward(geom, n_models, vel, wavelets, gathers, nullptr, 1, workspace, workspace_bytes, stream, geom->nt);
+}
+
 int32_t ss_gradient(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet,
                     const float* obs, const float* v_mute, float t_mute, float* grad, float* illum, void* workspace,
                     size_t workspace_bytes, void* stream) {
   return run_adjoint(SS_MODE_GRADIENT, geom, n_models, vel, wavelet, obs, v_mute, t_mute, 1.f, 0, nullptr, illum,
                      grad, workspace, workspace_bytes, stream);
+}
+
+int32_t ss_gradient_wavelets(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelets,
+                             const float* obs, const float* v_mute, float t_mute, float* grad, float* illum,
+                             void* workspace, size_t workspace_bytes, void* stream) {
+  if (!geom) return check_geometry(geom);
+  return run_adjoint(SS_MODE_GRADIENT, geom, n_models, vel, wavelets, obs, v_mute, t_mute, 1.f, 0, nullptr, illum,
+                     grad, workspace, workspace_bytes, stream, geom->nt);
 }
 
 int32_t ss_images(const ss_geometry* geom, int32_t n_models, const float* vel, const float* wavelet, const float* obs,

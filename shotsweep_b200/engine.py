@@ -84,12 +84,22 @@ class Engine:
         _lib.check(rc, 'device status')
 
     # -- entry points ----------------------------------------------------------
+    def _wavelet_in(self, wavelet, B):
+        """(wavelet, per_model): one wavelet [nt] for every model, or one per model [B, nt]."""
+        per_model = isinstance(wavelet, torch.Tensor) and wavelet.dim() == 2
+        shape = (B, self.g.nt) if per_model else (self.g.nt,)
+        return self._check_in(wavelet, shape, 'wavelet'), per_model
+
     def forward(self, vel, wavelet, ckpt_interval=None, out=None):
-        """Gathers [B, S, nt, nx] (+ checkpoints [B, S, n_ck, 2, nzp, nxp] if ckpt_interval)."""
+        """Gathers [B, S, nt, nx] (+ checkpoints [B, S, n_ck, 2, nzp, nxp] if ckpt_interval).
+
+        wavelet: [nt] for every model, or [B, nt] (one per model; no checkpoints)."""
         g = self.g
         B = vel.shape[0]
         vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
-        wavelet = self._check_in(wavelet, (g.nt,), 'wavelet')
+        wavelet, per_model = self._wavelet_in(wavelet, B)
+        if per_model and ckpt_interval:
+            raise ValueError('checkpoints are kept with one wavelet for every model only')
         if out is None:
             out = torch.empty(B, g.n_shots, g.nt, g.nx, dtype=torch.float32, device=self.device)
         ck = None
@@ -98,27 +108,33 @@ class Engine:
             ck = torch.zeros(B, g.n_shots, n_ck, 2, *self.padded, dtype=torch.float32, device=self.device)
         ws = self.workspace(B, _lib.MODE_FORWARD)
         with torch.cuda.device(self.device):
-            _lib.check(self.L.ss_forward(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(out),
-                                         _lib.ptr(ck), int(ckpt_interval or 0), _lib.ptr(ws), ws.numel(),
-                                         self._stream()), 'ss_forward')
+            if per_model:
+                _lib.check(self.L.ss_forward_wavelets(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet),
+                                                      _lib.ptr(out), _lib.ptr(ws), ws.numel(), self._stream()),
+                           'ss_forward_wavelets')
+            else:
+                _lib.check(self.L.ss_forward(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(out),
+                                             _lib.ptr(ck), int(ckpt_interval or 0), _lib.ptr(ws), ws.numel(),
+                                             self._stream()), 'ss_forward')
         return (out, ck) if ckpt_interval else out
 
     def gradient(self, vel, wavelet, obs, v_mute=None, t_mute=0.12):
-        """(grad, illum), each [B, S, nz, nx]."""
+        """(grad, illum), each [B, S, nz, nx]; wavelet [nt], or [B, nt] (one per model)."""
         g = self.g
         B = vel.shape[0]
         vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
-        wavelet = self._check_in(wavelet, (g.nt,), 'wavelet')
+        wavelet, per_model = self._wavelet_in(wavelet, B)
         obs = self._check_in(obs, (B, g.n_shots, g.nt, g.nx), 'obs')
         if v_mute is not None:
             v_mute = self._check_in(v_mute, (B,), 'v_mute')
         grad = torch.empty(B, g.n_shots, g.nz, g.nx, dtype=torch.float32, device=self.device)
         illum = torch.empty_like(grad)
         ws = self.workspace(B, _lib.MODE_GRADIENT)
+        entry = self.L.ss_gradient_wavelets if per_model else self.L.ss_gradient
         with torch.cuda.device(self.device):
-            _lib.check(self.L.ss_gradient(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(obs),
-                                          _lib.ptr(v_mute), float(t_mute), _lib.ptr(grad), _lib.ptr(illum),
-                                          _lib.ptr(ws), ws.numel(), self._stream()), 'ss_gradient')
+            _lib.check(entry(ctypes.byref(g), B, _lib.ptr(vel), _lib.ptr(wavelet), _lib.ptr(obs), _lib.ptr(v_mute),
+                             float(t_mute), _lib.ptr(grad), _lib.ptr(illum), _lib.ptr(ws), ws.numel(),
+                             self._stream()), 'ss_gradient_wavelets' if per_model else 'ss_gradient')
         return grad, illum
 
     def images_from_host(self, vel, wavelet, obs_host, v_mute=None, t_mute=0.12, eps=1e-4, laplacian=True,

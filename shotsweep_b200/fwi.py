@@ -13,6 +13,12 @@ shots, no mute) and its exact adjoint for the gradient of J = 0.5 sum (F(v) - d)
 
 Every model runs its own L-BFGS (its own history, step and stopping), batched
 in the kernels; only per-model scalars (misfits, g.d, steps) visit the host.
+
+``run_bands`` is the reference's multiscale loop (fwi.py:144-163): per frequency
+band (default a Gaussian low-pass at 8 Hz, then the full band) the gathers and
+the Ricker are low-passed, each model's source wavelet is estimated by a Wiener
+filter between its simulated and observed gathers (fwi.py:85-90), and L-BFGS
+runs with a fresh history, each model with its own wavelet.
 """
 from __future__ import annotations
 
@@ -24,9 +30,52 @@ import torch
 from . import _lib
 
 LO, HI = 1400.0, 4600.0
+BANDS, BAND_ITERS = (8.0, None), (10, 25)     # fwi.py:138
+
+
+def lowpass(x, fc, dt=1e-3):
+    """Gaussian low-pass exp(-0.5 (f/fc)^4) along the time axis (fwi.py:78-83), float64 FFTs.
+
+    x: gathers [..., nt, nx] on the device (returned float32) or a wavelet [nt] as a NumPy array
+    (returned float64).  fc None: x unchanged."""
+    if fc is None:
+        return x
+    if isinstance(x, torch.Tensor):
+        n = x.shape[-2]
+        f = torch.fft.rfftfreq(n, dt, dtype=torch.float64, device=x.device)
+        h = torch.exp(-0.5 * (f / fc) ** 4)
+        return torch.fft.irfft(torch.fft.rfft(x.double(), dim=-2) * h[:, None], n=n, dim=-2).float()
+    x = np.asarray(x, np.float64)
+    f = np.fft.rfftfreq(len(x), dt)
+    return np.fft.irfft(np.fft.rfft(x) * np.exp(-0.5 * (f / fc) ** 4), n=len(x))
+
+
+def estimate_wavelets(sim, obs, ricker, eps=1e-3):
+    """Each model's effective source (fwi.py:85-90): the Ricker shaped by the Wiener filter
+    sum conj(S) O / (sum |S|^2 + eps max) over the model's shots and receivers.
+
+    sim, obs: [B, S, nt, nx] on the device; ricker: [nt] (the wavelet `sim` was made with, unscaled).
+    Returns [B, nt] float64 on the device, unscaled."""
+    nt = sim.shape[2]
+    sf = torch.fft.rfft(sim.double(), dim=2)
+    of = torch.fft.rfft(obs.double(), dim=2)
+    num = (sf.conj() * of).sum(dim=(1, 3))
+    den = (sf.real ** 2 + sf.imag ** 2).sum(dim=(1, 3))
+    shaping = num / (den + eps * den.max(dim=1, keepdim=True).values)
+    r = torch.fft.rfft(torch.as_tensor(np.asarray(ricker, np.float64), device=sim.device))
+    return torch.fft.irfft(r[None] * shaping, n=nt, dim=1)
+
+
+def scaled(w):
+    """Injected samples: wavelet x 1e3 in float64, then float32 (gpu.py:94)."""
+    if isinstance(w, torch.Tensor):
+        return (w.double() * 1e3).float().contiguous()
+    return torch.as_tensor(np.asarray(w, np.float64) * 1e3, dtype=torch.float32)
 
 
 class BatchFWI:
+    """wavelet: scaled source samples [nt] for every model, or [B, nt] (one per model)."""
+
     def __init__(self, eng, wavelet, obs, mem=6, smooth=2.0, cap=50.0, c=1e-4, halvings=6):
         self.eng, self.w, self.obs = eng, wavelet, obs.contiguous()
         self.dev = eng.device
@@ -120,3 +169,29 @@ class BatchFWI:
                 callback(it, J)
         self.eng.status()
         return self.v.view(B, self.eng.g.nz, self.eng.g.nx).clone(), history
+
+    def run_bands(self, v0, ricker, bands=BANDS, iters=BAND_ITERS, eps=1e-3, callback=None):
+        """Multiscale FWI from v0 [B, nz, nx] (fwi.py:144-163).
+
+        ricker: the unscaled source wavelet [nt] that the bands are cut from.  Returns (v, history) with
+        history entries (seconds since the start, J per model, band index); J is the misfit against the
+        band's low-passed gathers, so only entries of one band compare."""
+        obs_full, w_full = self.obs, self.w
+        t0 = time.perf_counter()
+        history, v = [], v0
+        self.wavelets = []
+        try:
+            for k, (fc, nit) in enumerate(zip(bands, iters)):
+                self.obs = lowpass(obs_full, fc).contiguous()
+                ric = lowpass(ricker, fc)
+                sim = self.eng.forward(v.reshape(self.B, self.eng.g.nz, self.eng.g.nx).contiguous(),
+                                       scaled(ric).to(self.dev))
+                self.w = scaled(estimate_wavelets(sim, self.obs, ric, eps))
+                del sim
+                self.wavelets.append(self.w)
+                start = time.perf_counter() - t0          # the band's filtering and estimate included
+                v, h = self.run(v, nit, callback=callback)
+                history += [(start + t, J, k) for t, J in h]
+        finally:
+            self.obs, self.w = obs_full, w_full
+        return v, history

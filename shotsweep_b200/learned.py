@@ -1,6 +1,7 @@
 """Learned proposal + FWI: train on simulator gathers, propose, accept by forward misfit, refine by L-BFGS.
 
-    res = run(n_train=20000, n_test=256, steps=6000, iters=50)
+    res = run(n_train=20000, n_test=256, steps=6000, iters=50)                 # one full band
+    res = run(..., iters=(10, 25), bands=(8.0, None))                           # the reference's two bands
 
 1. Training data: `n_train` seeded models from the synthetic families (an equal mix of
    layered, curved, faulted and textured), their gathers simulated by the library's
@@ -14,9 +15,12 @@
    background.py:97-99; the training models' mean surface velocity where the picker refuses).
 4. Acceptance by forward misfit: each model starts FWI from the proposal if its data misfit is
    below the background's, otherwise from the background (the fallback is plain FWI).
-5. ``fwi.BatchFWI`` from both starts for `iters` L-BFGS iterations; the time-to-misfit is the
-   wall time the learned start (inference and acceptance included) needs to reach the final
-   total misfit of plain FWI from the background, against plain FWI's own wall time.
+5. ``fwi.BatchFWI.run_bands`` from both starts: L-BFGS for `iters` iterations in the full band
+   (an int), or the reference's multiscale schedule (fwi.py:138-163: `bands` such as an 8 Hz
+   low-pass then the full band, `iters` per band, each model with its own Wiener-estimated wavelet
+   per band).  The time-to-misfit is the wall time the learned start (inference and acceptance
+   included) needs to reach plain FWI's final full-band total misfit, against plain FWI's own wall
+   time; only full-band misfits are compared.
 """
 from __future__ import annotations
 
@@ -96,7 +100,8 @@ def norm_mae(v, truth):
     return float(np.abs(a - b).mean())
 
 
-def run(n_train=20000, n_test=256, steps=6000, batch=64, iters=50, seed=0, train_tag=101, test_tag=202, log=print):
+def run(n_train=20000, n_test=256, steps=6000, batch=64, iters=50, bands=None, seed=0, train_tag=101,
+        test_tag=202, log=print):
     dev = torch.device('cuda', torch.cuda.current_device())
     sim = gpu.Sim(device=dev)
     eng = sim.engine
@@ -140,13 +145,18 @@ def run(n_train=20000, n_test=256, steps=6000, batch=64, iters=50, seed=0, train
                propose_seconds=propose_s,
                mae_background=norm_mae(bg.cpu().numpy(), test_models),
                mae_proposal=norm_mae(prop.cpu().numpy(), test_models))
-    v_plain, h_plain = BatchFWI(eng, w, obs).run(bg, iters)
-    v_learn, h_learn = BatchFWI(eng, w, obs).run(start, iters)
-    plain_total = [float(h[1].sum()) for h in h_plain]
-    learn_total = [float(h[1].sum()) for h in h_learn]
+    if isinstance(iters, int):             # one full band
+        bands, iters = (None,), (iters,)
+    if bands is None or len(bands) != len(iters):
+        raise ValueError('give one iteration count per band')
+    v_plain, h_plain = BatchFWI(eng, w, obs).run_bands(bg, gpu.RICKER, bands, iters)
+    v_learn, h_learn = BatchFWI(eng, w, obs).run_bands(start, gpu.RICKER, bands, iters)
+    last = len(bands) - 1
+    plain_total = [float(h[1].sum()) for h in h_plain if h[2] == last]
+    learn_total = [float(h[1].sum()) for h in h_learn if h[2] == last]
     target = plain_total[-1]
     t_plain = h_plain[-1][0]
-    reach = next((propose_s + h[0] for h, J in zip(h_learn, learn_total) if J <= target), None)
+    reach = next((propose_s + h[0] for h in h_learn if h[2] == last and float(h[1].sum()) <= target), None)
     res.update(plain_final_misfit=target, learned_final_misfit=learn_total[-1], plain_seconds=t_plain,
                learned_seconds=h_learn[-1][0] + propose_s, learned_time_to_plain_misfit=reach,
                time_ratio=None if reach is None else reach / t_plain,
