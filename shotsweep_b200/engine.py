@@ -146,9 +146,10 @@ class Engine:
         return to pinned host memory on a second copy stream behind each chunk.  The chunks grow from one
         round of the persistent clusters, so that imaging starts after a short first copy, and the last one
         is small, so that little is left to copy back at the end: a call costs about the imaging time.
-        vel: [B, nz, nx] float32, on the device or on the host (pinned or not).  obs_host: CPU tensor
-        [B, S, nt, nx] float32, pinned or not (pageable rows are staged through pinned buffers).
-        `chunk_rows` fixes a uniform chunk size instead.
+        vel: [B, nz, nx], float32 on the device, or float32 / float64 on the host (each chunk's rows are
+        converted into a pinned float32 buffer just before its copy, while the previous chunk is imaged).
+        obs_host: CPU tensor [B, S, nt, nx] float32, pinned or not (pageable rows are staged through pinned
+        buffers).  `chunk_rows` fixes a uniform chunk size instead.
         """
         g = self.g
         B = vel.shape[0]
@@ -162,9 +163,9 @@ class Engine:
         f32 = dict(dtype=torch.float32, device=dev)
         host_vel = isinstance(vel, torch.Tensor) and vel.device.type == 'cpu'
         if host_vel:
-            if vel.dtype != torch.float32 or tuple(vel.shape) != (B, g.nz, g.nx):
-                raise ValueError(f'vel must be a float32 tensor of shape {(B, g.nz, g.nx)}')
-            vel_host = vel.contiguous() if vel.is_pinned() else vel.contiguous().pin_memory()
+            if vel.dtype not in (torch.float32, torch.float64) or tuple(vel.shape) != (B, g.nz, g.nx):
+                raise ValueError(f'vel must be a float32 or float64 tensor of shape {(B, g.nz, g.nx)}')
+            vel_host = vel.contiguous()
             vel = torch.empty(B, g.nz, g.nx, **f32)
         else:
             vel = self._check_in(vel, (B, g.nz, g.nx), 'vel')
@@ -180,6 +181,8 @@ class Engine:
         pinned = obs_host.is_pinned()
         staging = [] if pinned else [torch.empty(chunk, *shape[1:], dtype=torch.float32, pin_memory=True)
                                      for _ in range(min(2, n_chunks))]
+        vel_staging = [torch.empty(chunk, g.nz, g.nx, dtype=torch.float32, pin_memory=True)
+                       for _ in range(min(2, n_chunks))] if host_vel else []
         img_dev = torch.empty(B, g.n_shots, g.nz, g.nx, **f32)
         illum_dev = torch.empty_like(img_dev)
         img = torch.empty(img_dev.shape, dtype=torch.float32, pin_memory=True)
@@ -190,17 +193,19 @@ class Engine:
         for k, (a, b) in enumerate(bounds):
             buf = k % len(dev_obs)
             src = obs_host[a:b]
+            if (not pinned or host_vel) and k >= len(dev_obs):
+                copied[buf].synchronize()              # the staging buffers' previous rows have left
             if not pinned:
-                if k >= len(staging):
-                    copied[buf].synchronize()          # the staging buffer's previous rows have left
                 staging[buf][:b - a].copy_(src)
                 src = staging[buf][:b - a]
+            if host_vel:
+                vel_staging[buf][:b - a].copy_(vel_host[a:b])
             with torch.cuda.stream(h2d):
                 if k >= len(dev_obs):
                     h2d.wait_event(imaged[buf])        # the device buffer's previous chunk is imaged
                 dev_obs[buf][:b - a].copy_(src, non_blocking=True)
                 if host_vel:
-                    vel[a:b].copy_(vel_host[a:b], non_blocking=True)
+                    vel[a:b].copy_(vel_staging[buf][:b - a], non_blocking=True)
                 copied[buf].record(h2d)
             compute.wait_event(copied[buf])
             self.images(vel[a:b], wavelet, dev_obs[buf][:b - a], None if v_mute is None else v_mute[a:b], t_mute, eps,

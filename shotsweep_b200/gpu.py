@@ -228,11 +228,9 @@ class Sim:
             o = o.to(torch.float32) if o.dtype != torch.float32 else o
             if tuple(o.shape) != (B, 5, NT, NX):                                   # gpu.py:156-157
                 raise ValueError(f'observations must be finite with shape {(B, 5, NT, NX)}')
-            vh = torch.empty(v.shape, dtype=torch.float32, pin_memory=True)   # model rows follow their chunks
-            vh.copy_(torch.from_numpy(v))
-            try:
-                img, illum = self.engine.images_from_host(vh, self._wavelet(), o, self._mute(v_mute, B),
-                                                          t_mute, eps, laplacian)
+            try:   # float64 model rows are converted and copied chunk by chunk
+                img, illum = self.engine.images_from_host(torch.from_numpy(v), self._wavelet(), o,
+                                                          self._mute(v_mute, B), t_mute, eps, laplacian)
             except ValueError:
                 raise ValueError(f'observations must be finite with shape {(B, 5, NT, NX)}') from None
             return img.numpy(), illum.numpy()

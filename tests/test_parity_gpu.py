@@ -132,8 +132,8 @@ def test_batch_larger_than_resident_clusters_is_deterministic(gpu):
 
 
 def test_host_pipeline_equals_device_images(gpu):
-    """The chunked host-observation pipeline (device or host velocities, pinned or pageable gathers, uniform
-    or growing chunks) gives the device-resident images bit for bit."""
+    """The chunked host-observation pipeline (device velocities, or float32 / float64 host velocities; pinned
+    or pageable gathers; uniform or growing chunks) gives the device-resident images bit for bit."""
     from shotsweep_b200 import engine, synth
     sim = gpu.Sim()
     eng = sim.engine
@@ -146,7 +146,8 @@ def test_host_pipeline_equals_device_images(gpu):
     ref_img, ref_illum = eng.images(bgs.to(eng.device), w, obs.to(eng.device), vm, 0.12)
     eng.status()
     assert [b - a for a, b in eng._chunks(30)][:2] == [9, 18]
-    for vel, o, rows in ((bgs, obs.pin_memory(), None), (bgs.to(eng.device), obs, 7), (bgs.pin_memory(), obs, None)):
+    for vel, o, rows in ((bgs, obs.pin_memory(), None), (bgs.to(eng.device), obs, 7), (bgs.pin_memory(), obs, None),
+                         (bgs.double(), obs.pin_memory(), 4)):
         img, illum = eng.images_from_host(vel, w, o, vm, 0.12, chunk_rows=rows)
         assert torch.equal(img, ref_img.cpu()) and torch.equal(illum, ref_illum.cpu())
 
