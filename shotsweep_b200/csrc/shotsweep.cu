@@ -4,7 +4,9 @@
 // cluster of C CTAs (C = 3 for the 150x150 padded OpenFWI grid); the padded grid
 // is cut into C horizontal bands, one per CTA.  Each thread keeps a 5 x 4 tile
 // of both time levels in registers for the whole time loop; shared memory holds
-// the current level of the band for the neighbouring tiles' stencils.
+// the current level of the band for the neighbouring tiles' stencils, and the
+// tile's per-cell coefficients sit in tensor memory (TMEM), read row by row
+// with tcgen05.ld, which leaves the registers to the wavefields.
 // Neighbouring bands push their two edge rows into each other's halo rows every
 // step through distributed shared memory (st.async counted on mbarriers).
 //
@@ -52,6 +54,11 @@ constexpr int kMinTraceRing = 8;           // the fewest, for grids whose shared
 constexpr int kStages = 3;                 // history slabs in flight: prefetch / retire depth kStages-1
 constexpr int kFastRS = 156;               // shared row stride of the 150-column padded OpenFWI grid
 constexpr size_t kMaxSmem = 227 * 1024;
+// The fixed-geometry kernels allocate kCoefCols of an SM's 512 tensor-memory
+// columns per CTA.  At least 60 KB of shared memory per CTA keeps three or
+// fewer of them on one SM (228 KB), so every allocation is served at once and
+// no CTA waits for columns held by a CTA that waits for it.
+constexpr size_t kTcMinSmem = 60 * 1024;
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s per bounded wait
 
 thread_local std::string g_last_error;
@@ -95,6 +102,44 @@ __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+
+// Tensor memory (TMEM) holds the per-cell coefficients of the fixed-geometry
+// kernels: warp w may reach lanes 32*(w%4) .. +31 only, so thread (w, l) owns
+// lane 32*(w%4) + l and columns kCoefColsPerWarp*(w/4) + 8k .. +7 for tile row
+// k: kappa (4 cells), then -sigma (4 cells).
+constexpr uint32_t kCoefColsPerWarp = 40;   // 5 tile rows x 8 words
+constexpr uint32_t kCoefCols = 128;         // 3 warp groups x 40, as a power of two
+__device__ __forceinline__ void tmem_alloc_warp(uint32_t dst_smem, uint32_t ncols) {   // one whole warp
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_warp(uint32_t taddr, uint32_t ncols) {   // the allocating warp
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 8 consecutive 32-bit columns of this thread's lane (whole warp, converged).
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+               "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+// Starts loading 8 columns; the registers are valid after tmem_wait_ld on them.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+               : "r"(taddr)
+               : "memory");
+}
+// Completes this thread's TMEM loads; the operands order every later use of v after it.
+__device__ __forceinline__ void tmem_wait_ld(float (&v)[8]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7])
+               :
+               : "memory");
 }
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
@@ -362,6 +407,27 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
 }
 
 
+// Coefficients of tile row k: ck0, ck1 (kappa) and cs0, cs1 (-sigma), each
+// for two cells; from registers, or (TC) loaded from tensor memory at the
+// row.  (Loading the next row one row ahead keeps 8 more registers live and
+// measured slower.)
+#define SS_COEF_ROW(k) \
+          float2 ck0, ck1, cs0, cs1; \
+          if constexpr (TC) { \
+            float cfr[8]; \
+            tmem_ld8(tc_base + 8u * (k), cfr); \
+            tmem_wait_ld(cfr); \
+            ck0 = make_float2(cfr[0], cfr[1]); \
+            ck1 = make_float2(cfr[2], cfr[3]); \
+            cs0 = make_float2(cfr[4], cfr[5]); \
+            cs1 = make_float2(cfr[6], cfr[7]); \
+          } else { \
+            ck0 = kap[k][0]; \
+            ck1 = kap[k][1]; \
+            cs0 = nsig[k][0]; \
+            cs1 = nsig[k][1]; \
+          }
+
 // Body of one tile row k (a compile-time constant after unrolling) inside
 // solve_kernel's step; written once, expanded in two row orders, each with
 // (SPECIAL) and without the source / receiver terms.
@@ -375,8 +441,8 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
           const float2 rt = *reinterpret_cast<const float2*>(xc + (k + 2) * RS + 4); \
           float2 s_lo, s_hi; \
           neg_stencil(rm2, rm1, rc, rp1, rp2, lf, rt, s_lo, s_hi); \
-          const float2 n_lo = leapfrog(kap[k][0], nsig[k][0], O1[k][0], O2[k][0], s_lo); \
-          const float2 n_hi = leapfrog(kap[k][1], nsig[k][1], O1[k][1], O2[k][1], s_hi); \
+          const float2 n_lo = leapfrog(ck0, cs0, O1[k][0], O2[k][0], s_lo); \
+          const float2 n_hi = leapfrog(ck1, cs1, O1[k][1], O2[k][1], s_hi); \
           float4 nw = make_float4(n_lo.x, n_lo.y, n_hi.x, n_hi.y); \
           if (fwd) { \
             if (SPECIAL) {  /* injection after damping (gpu.py:113-114) */ \
@@ -393,10 +459,10 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
               const bool on = k == rec_k; \
               const float r0v = rs[min(max(rr, 0), NX - 1)], r1v = rs[min(max(rr + 1, 0), NX - 1)]; \
               const float r2v = rs[min(max(rr + 2, 0), NX - 1)], r3v = rs[min(max(rr + 3, 0), NX - 1)]; \
-              nw.x = fmaf((on && rr >= 0 && rr < NX) ? -nsig[k][0].x : 0.f, r0v, nw.x); \
-              nw.y = fmaf((on && rr + 1 >= 0 && rr + 1 < NX) ? -nsig[k][0].y : 0.f, r1v, nw.y); \
-              nw.z = fmaf((on && rr + 2 >= 0 && rr + 2 < NX) ? -nsig[k][1].x : 0.f, r2v, nw.z); \
-              nw.w = fmaf((on && rr + 3 >= 0 && rr + 3 < NX) ? -nsig[k][1].y : 0.f, r3v, nw.w); \
+              nw.x = fmaf((on && rr >= 0 && rr < NX) ? -cs0.x : 0.f, r0v, nw.x); \
+              nw.y = fmaf((on && rr + 1 >= 0 && rr + 1 < NX) ? -cs0.y : 0.f, r1v, nw.y); \
+              nw.z = fmaf((on && rr + 2 >= 0 && rr + 2 < NX) ? -cs1.x : 0.f, r2v, nw.z); \
+              nw.w = fmaf((on && rr + 3 >= 0 && rr + 3 < NX) ? -cs1.y : 0.f, r3v, nw.w); \
             } \
             if (SPECIAL) {  /* source-strength term (gpu.py:182) */ \
               const float a = (k == src_k) ? wt : 0.f; \
@@ -455,6 +521,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 #define GNSEG (BATCH ? gs.nseg : P.nseg)
 #define GNACT (BATCH ? gs.nact : P.nact)
 
+  // The fixed-geometry instantiations keep the per-cell coefficients in
+  // tensor memory (freeing 40 registers per thread); the uneven batch keeps
+  // them in registers.
+  constexpr bool TC = !BATCH;
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
   // A 1-D grid of 1-D clusters: the CTA's rank in its cluster and the
@@ -496,6 +566,11 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     for (int b = 0; b < kStages + 2; ++b) mbar_init(smem_u32(&S.bar[b]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  // kCoefCols TMEM columns, allocated by warp 0; the address lands in the
+  // word after the barriers.  The planner keeps at most three CTAs of this
+  // kernel on an SM, so the allocation never waits on another CTA.
+  if (TC && tid < 32) tmem_alloc_warp(smem_u32(&S.bar[kStages + 2]), kCoefCols);
+  if (TC) tmem_fence_before();
   const uint32_t hist_bar0 = smem_u32(&S.bar[0]);
   const uint32_t halo_bar0 = smem_u32(&S.bar[kStages]);
   uint32_t hist_phase = 0, halo_phase = 0;   // parity of the next wait, one bit per buffer
@@ -508,6 +583,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
   const size_t trace_slot = BATCH ? P.trace_slot : static_cast<size_t>(P.nt) * NXS;
 
   cluster_sync();   // barriers initialised and wavelet staged everywhere
+  uint32_t tc_base = 0;   // this thread's TMEM lane and first coefficient column
+  if (TC) {
+    tmem_fence_after();
+    const uint32_t warp = static_cast<uint32_t>(tid >> 5);
+    tc_base = *reinterpret_cast<const uint32_t*>(&S.bar[kStages + 2]) + ((32u * (warp & 3u)) << 16) +
+              kCoefColsPerWarp * (warp >> 2);
+  }
 
   for (int it = slot;; it += n_slots) {
     // ---- next solve: round robin, or (uneven batch) the next entry of the
@@ -624,6 +706,15 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
                                  : nullptr;
 
     // ---- per-cell coefficients ----------------------------------------
+    // kappa = 2A and -sigma = -(c2 A)/12 of every cell: in tensor memory
+    // (TC; the source cell's -sigma also stays in a register for the
+    // gradient's source term) or in registers.
+    int src_k = -1, src_m = 0;
+    if (active && src_r >= myrow && src_r < myrow + H && src_c >= col0 && src_c < col0 + 4) {
+      src_k = src_r - myrow;
+      src_m = src_c - col0;
+    }
+    float nsig_src = 0.f;
     float2 kap[H][2], nsig[H][2], acc[H][2], A[H][2], B[H][2];
 #pragma unroll
     for (int k = 0; k < H; ++k) {
@@ -643,18 +734,20 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         }
         kvs[m] = kv;
         svs[m] = sv;
+        if (TC && k == src_k && m == src_m) nsig_src = sv;
       }
-      kap[k][0] = make_float2(kvs[0], kvs[1]);
-      kap[k][1] = make_float2(kvs[2], kvs[3]);
-      nsig[k][0] = make_float2(svs[0], svs[1]);
-      nsig[k][1] = make_float2(svs[2], svs[3]);
+      if (TC) {
+        const float cf[8] = {kvs[0], kvs[1], kvs[2], kvs[3], svs[0], svs[1], svs[2], svs[3]};
+        tmem_st8(tc_base + 8u * k, cf);
+      } else {
+        kap[k][0] = make_float2(kvs[0], kvs[1]);
+        kap[k][1] = make_float2(kvs[2], kvs[3]);
+        nsig[k][0] = make_float2(svs[0], svs[1]);
+        nsig[k][1] = make_float2(svs[2], svs[3]);
+      }
       acc[k][0] = acc[k][1] = A[k][0] = A[k][1] = B[k][0] = B[k][1] = make_float2(0.f, 0.f);
     }
-    int src_k = -1, src_m = 0;
-    if (active && src_r >= myrow && src_r < myrow + H && src_c >= col0 && src_c < col0 + 4) {
-      src_k = src_r - myrow;
-      src_m = src_c - col0;
-    }
+    if (TC) tmem_wait_st();
     // Halo rows are pushed inside the row loop.  Injections and the source
     // term are needed only by warps that hold a receiver (or source) cell:
     // the step branches once on this warp-uniform flag into a row loop with
@@ -768,11 +861,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 #pragma unroll
             for (int i = 0; i < H; ++i) {
               const int k = H - 1 - i;
+              SS_COEF_ROW(k)
               SS_TILE_ROW(k, true)
             }
           } else {
 #pragma unroll
             for (int k = 0; k < H; ++k) {
+              SS_COEF_ROW(k)
               SS_TILE_ROW(k, true)
             }
           }
@@ -781,11 +876,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 #pragma unroll
             for (int i = 0; i < H; ++i) {
               const int k = H - 1 - i;
+              SS_COEF_ROW(k)
               SS_TILE_ROW(k, false)
             }
           } else {
 #pragma unroll
             for (int k = 0; k < H; ++k) {
+              SS_COEF_ROW(k)
               SS_TILE_ROW(k, false)
             }
           }
@@ -987,7 +1084,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
             float gval = -2.f * a / vp;
             if (k == src_k && m == src_m) {
               const float deriv = static_cast<float>(2.0 * v_src / (P.amp_ref * P.amp_ref));
-              const float ns = (m & 1) ? nsig[k][m >> 1].y : nsig[k][m >> 1].x;
+              const float ns = TC ? nsig_src : ((m & 1) ? nsig[k][m >> 1].y : nsig[k][m >> 1].x);
               gval += src_acc * deriv / -ns;
             }
             gp[static_cast<size_t>(r) * GNXP + c] = gval;
@@ -1004,7 +1101,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     __threadfence();
     cluster_sync();   // scratch of this slot is free for the next solve
   }
+  if (TC) tmem_fence_before();
   cluster_sync();     // no CTA leaves while a neighbour may still write its shared memory
+  if (TC && tid < 32) {
+    tmem_fence_after();
+    tmem_dealloc_warp(*reinterpret_cast<const uint32_t*>(&S.bar[kStages + 2]), kCoefCols);
+  }
 }
 
 #undef RS
@@ -1254,7 +1356,7 @@ size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring) {
   return (2 * field + kStages * stage + ((nt + 31) & ~31) + 32 + (kStages + ring) * static_cast<size_t>(nxs) +
           (kRowsPerThread + 4) * static_cast<size_t>(rs) + kRowsPerThread * static_cast<size_t>(sw)) *
              sizeof(float) +
-         (kStages + 2) * sizeof(uint64_t);
+         (kStages + 3) * sizeof(uint64_t);   // barriers, then the TMEM address word
 }
 
 int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
@@ -1290,6 +1392,7 @@ int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
   }
   if (!ok) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits shared memory for this grid");
   p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
+  p->smem = std::max(p->smem, kTcMinSmem);
   p->fast = fast_geometry(g->nx, g->pad);
   const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->fast));
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->smem));
