@@ -695,6 +695,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     // so that the rows pushed to the next band are ready early in the step;
     // the order is uniform per warp (the tile is in registers, any order works).
     const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
+    // Warp-uniform forms of per-thread conditions of the step (votes, which
+    // the compiler knows are uniform): the branches they guard need no
+    // reconvergence in the warps that skip them.
+    const bool warp_edge = __any_sync(0xffffffffu, edge_up || edge_dn);
+    const bool warp0 = __any_sync(0xffffffffu, tid == 0);
+    const bool warp_recv = __any_sync(0xffffffffu, tid < NX);
 
     const uint32_t stage_bytes = static_cast<uint32_t>(static_cast<size_t>(GBH) * SW * sizeof(float));
     const size_t hist_slot = BATCH ? P.hist_slot : static_cast<size_t>(P.hist_steps) * hist_step_fixed;
@@ -789,7 +795,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       float* Y = cur ? S.f[0] : S.f[1];
       const bool more = step + 1 < n_steps;
       const int bi = lvl % kStages;
-      if (tid == 0 && more) {
+      if (warp0 && more && tid == 0) {
         if (halo_bytes) mbar_expect_tx(halo_bar0 + 8u * (cur ^ 1), halo_bytes);
         if (!fwd && lvl - (kStages - 1) >= lvl_lo) {   // history slab (and residual row) kStages-1 steps ahead
           const int tn = lvl - (kStages - 1), bn = tn % kStages;
@@ -818,20 +824,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           }
         }
       }
-      if ((edge_up || edge_dn) && step > 0) {
-        mbar_wait_bounded(halo_bar0 + 8u * cur, (halo_phase >> cur) & 1u, P.err);
-        if (!BATCH) halo_phase ^= 1u << cur;
-      }
-      // A halo barrier completes one phase per step after the first.  In a
-      // batch the edge threads change from solve to solve, so every thread
-      // follows the phases, waiting or not.
-      if (BATCH && step > 0) halo_phase ^= 1u << cur;
+      // A halo barrier completes one phase per step after the first; every
+      // thread follows the phases, and every thread of a warp that holds an
+      // edge tile waits (the other lanes would wait for their warp anyway).
+      if (warp_edge && step > 0) mbar_wait_bounded(halo_bar0 + 8u * cur, (halo_phase >> cur) & 1u, P.err);
+      if (step > 0) halo_phase ^= 1u << cur;
       if (!fwd) {
         mbar_wait_bounded(hist_bar0 + 8u * bi, (hist_phase >> bi) & 1u, P.err);
         hist_phase ^= 1u << bi;
       }
       const bool push_up = more && edge_up, push_dn = more && edge_dn;
-      if (!SEG && fwd && rank == rec_rank && step > 0) {
+      if (!SEG && fwd && rank == rec_rank && step > 0 && warp_recv) {
         // receivers at every model column (gpu.py:134): the level recorded at
         // the previous step is now the read-only field X
         #pragma unroll 1
@@ -890,10 +893,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
       }
       if (fwd && ADJ) {
         fence_proxy_async_smem();
-        if (tid == 0 && step > 0) bulk_wait_read_lag();   // the slab to be refilled next step has left shared memory
+        if (warp0 && step > 0 && tid == 0) bulk_wait_read_lag();   // the slab to be refilled next step has left shared memory
       }
       __syncthreads();
-      if (fwd && ADJ && tid == 0)
+      if (fwd && ADJ && warp0 && tid == 0)
         bulk_store(hist_mine + static_cast<size_t>(lvl - lvl_lo) * hist_step, smem_u32(stage_buf(bi)), stage_bytes);
       if (!SEG && fwd && rank == rec_rank) {
         // The ring holds the receiver rows [flushed, lvl-1] (level lvl-1 was
