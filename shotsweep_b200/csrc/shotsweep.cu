@@ -808,7 +808,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           if (res_here) bulk_load(smem_u32(res_buf(bn)), trace + static_cast<size_t>(tn) * NXS, res_bytes, bar);
         }
       }
-      if (!BATCH && MODE == SS_MODE_FORWARD && fwd && P.ckpt != nullptr && lvl % P.ckpt_interval == 0 && active) {
+      if (!BATCH && MODE == SS_MODE_FORWARD && fwd && P.ckpt != nullptr && lvl % P.ckpt_interval == 0) {
         float* ck = P.ckpt + ((static_cast<size_t>(solve) * P.n_ckpt + lvl / P.ckpt_interval) * 2) * P.nzp * P.nxp;
 #pragma unroll
         for (int k = 0; k < H; ++k) {
@@ -816,7 +816,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 #pragma unroll
           for (int m = 0; m < 4; ++m) {
             const int c = col0 + m;
-            if (r < P.nzp - 2 && c < P.nxp - 2) {
+            if (active && r < P.nzp - 2 && c < P.nxp - 2) {   // per-thread test inside the uniform branch
               const float2 o2 = O2[k][m >> 1], o1 = O1[k][m >> 1];
               ck[static_cast<size_t>(r) * P.nxp + c] = (m & 1) ? o2.y : o2.x;
               ck[static_cast<size_t>(P.nzp) * P.nxp + static_cast<size_t>(r) * P.nxp + c] = (m & 1) ? o1.y : o1.x;
