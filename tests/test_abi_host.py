@@ -102,6 +102,24 @@ def test_memory_model_is_bounded():
     assert gpu.imaging_memory_bytes(1) < gpu.imaging_memory_bytes(300)
 
 
+def test_host_pipeline_chunks_cover_rows_in_whole_rounds():
+    """The host-observation pipeline's chunks: contiguous, covering every row once, whole rounds of the
+    persistent clusters except the last, growing x6 from one round, capped at a third of the rows and 1 GiB."""
+    from shotsweep_b200 import engine
+    eng = engine.Engine.__new__(engine.Engine)          # host logic only: no device
+    eng.g = engine.geometry()
+    eng.plan = lambda n_models, mode: {'slots': 45}
+    per_round = 9                                        # 45 clusters / 5 shots
+    for B in (1, 8, 9, 10, 48, 100, 1500, 20000):
+        ch = eng._chunks(B)
+        assert ch[0][0] == 0 and ch[-1][1] == B
+        assert all(a2 == b1 for (_, b1), (a2, _) in zip(ch, ch[1:])) and all(b > a for a, b in ch)
+        assert all((b - a) % per_round == 0 for a, b in ch[:-1])
+        assert max(b - a for a, b in ch) * 5 * 1000 * 70 * 4 <= max(1 << 30, per_round * 5 * 1000 * 70 * 4)
+    assert [(b - a) // per_round for a, b in eng._chunks(1500)][:4] == [1, 6, 36, 56]
+    assert eng._chunks(100, chunk_rows=30) == [(0, 30), (30, 60), (60, 90), (90, 100)]
+
+
 def test_struct_layouts_match_the_header(tmp_path):
     """The ctypes mirrors have the sizes and field offsets that a C compiler gives the header's structs."""
     import ctypes
