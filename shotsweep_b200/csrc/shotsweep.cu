@@ -453,16 +453,12 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
               nw.w += (src_m == 3) ? a : 0.f; \
             } \
           } else { \
-            if (SPECIAL) {  /* residual injection th += sigma*res (gpu.py:180) */ \
-              const float* rs = res_buf(bi); \
-              const int rr = col0 - PAD; \
+            if (SPECIAL) {  /* residual injection th += sigma*res (gpu.py:180), res loaded once per step */ \
               const bool on = k == rec_k; \
-              const float r0v = rs[min(max(rr, 0), NX - 1)], r1v = rs[min(max(rr + 1, 0), NX - 1)]; \
-              const float r2v = rs[min(max(rr + 2, 0), NX - 1)], r3v = rs[min(max(rr + 3, 0), NX - 1)]; \
-              nw.x = fmaf((on && rr >= 0 && rr < NX) ? -cs0.x : 0.f, r0v, nw.x); \
-              nw.y = fmaf((on && rr + 1 >= 0 && rr + 1 < NX) ? -cs0.y : 0.f, r1v, nw.y); \
-              nw.z = fmaf((on && rr + 2 >= 0 && rr + 2 < NX) ? -cs1.x : 0.f, r2v, nw.z); \
-              nw.w = fmaf((on && rr + 3 >= 0 && rr + 3 < NX) ? -cs1.y : 0.f, r3v, nw.w); \
+              nw.x = fmaf(on ? -cs0.x : 0.f, rv0, nw.x); \
+              nw.y = fmaf(on ? -cs0.y : 0.f, rv1, nw.y); \
+              nw.z = fmaf(on ? -cs1.x : 0.f, rv2, nw.z); \
+              nw.w = fmaf(on ? -cs1.y : 0.f, rv3, nw.w); \
             } \
             if (SPECIAL) {  /* source-strength term (gpu.py:182) */ \
               const float a = (k == src_k) ? wt : 0.f; \
@@ -859,7 +855,18 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         // that the halo push to the next band leaves early in the step.  The
         // source and receiver terms are compiled into the rows of the first
         // branch only (one warp-uniform branch per step instead of one per row).
+        // Adjoint, receiver warps: this step's residual at the tile's four
+        // columns (zero off the receiver columns), read once for all rows.
+        float rv0 = 0.f, rv1 = 0.f, rv2 = 0.f, rv3 = 0.f;
         if (warp_special) {
+          if (!fwd) {
+            const float* rs = res_buf(bi);
+            const int rr = col0 - PAD;
+            rv0 = (rr >= 0 && rr < NX) ? rs[min(max(rr, 0), NX - 1)] : 0.f;
+            rv1 = (rr + 1 >= 0 && rr + 1 < NX) ? rs[min(max(rr + 1, 0), NX - 1)] : 0.f;
+            rv2 = (rr + 2 >= 0 && rr + 2 < NX) ? rs[min(max(rr + 2, 0), NX - 1)] : 0.f;
+            rv3 = (rr + 3 >= 0 && rr + 3 < NX) ? rs[min(max(rr + 3, 0), NX - 1)] : 0.f;
+          }
           if (rev_rows) {
 #pragma unroll
             for (int i = 0; i < H; ++i) {
