@@ -445,12 +445,12 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
           const float2 n_hi = leapfrog(ck1, cs1, O1[k][1], O2[k][1], s_hi); \
           float4 nw = make_float4(n_lo.x, n_lo.y, n_hi.x, n_hi.y); \
           if (fwd) { \
-            if (SPECIAL) {  /* injection after damping (gpu.py:113-114) */ \
-              const float a = (k == src_k) ? wt : 0.f; \
-              nw.x += (src_m == 0) ? a : 0.f; \
-              nw.y += (src_m == 1) ? a : 0.f; \
-              nw.z += (src_m == 2) ? a : 0.f; \
-              nw.w += (src_m == 3) ? a : 0.f; \
+            if (SPECIAL) {  /* injection after damping (gpu.py:113-114): + w at the source cell */ \
+              const float on = (k == src_k) ? 1.f : 0.f; \
+              nw.x = fmaf(on, am0, nw.x); \
+              nw.y = fmaf(on, am1, nw.y); \
+              nw.z = fmaf(on, am2, nw.z); \
+              nw.w = fmaf(on, am3, nw.w); \
             } \
           } else { \
             if (SPECIAL) {  /* residual injection th += sigma*res (gpu.py:180), res loaded once per step */ \
@@ -857,8 +857,16 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         // branch only (one warp-uniform branch per step instead of one per row).
         // Adjoint, receiver warps: this step's residual at the tile's four
         // columns (zero off the receiver columns), read once for all rows.
+        // Forward: this step's source amount at each of the tile's columns.
         float rv0 = 0.f, rv1 = 0.f, rv2 = 0.f, rv3 = 0.f;
+        float am0 = 0.f, am1 = 0.f, am2 = 0.f, am3 = 0.f;
         if (warp_special) {
+          if (fwd) {
+            am0 = (src_m == 0) ? wt : 0.f;
+            am1 = (src_m == 1) ? wt : 0.f;
+            am2 = (src_m == 2) ? wt : 0.f;
+            am3 = (src_m == 3) ? wt : 0.f;
+          }
           if (!fwd) {
             const float* rs = res_buf(bi);
             const int rr = col0 - PAD;
