@@ -23,9 +23,9 @@
 // and mu at the source is th/sigma there (gpu.py:181-187).
 //
 // Instead of the reference's checkpoint-and-recompute (gpu.py:131,169-176) the
-// forward stores S(p[t]) of every step to a per-cluster history in HBM with
-// TMA bulk copies (cp.async.bulk) and the adjoint streams it back in reverse,
-// prefetching two steps ahead.  This trades 2x4 bytes of HBM traffic per cell
+// forward stores S(p[t]) of every step to a per-cluster history in HBM
+// (coalesced 16-byte stores from every thread) and the adjoint streams it
+// back in reverse with TMA bulk copies (cp.async.bulk), two steps ahead.  This trades 2x4 bytes of HBM traffic per cell
 // and step for the 16 flops per cell and step that a recompute would cost.
 
 #include <cuda_runtime.h>
@@ -173,20 +173,6 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
-}
-__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
-               : "memory");
-  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-}
-// At most kStages-2 newer history stores may still be reading shared memory.
-__device__ __forceinline__ void bulk_wait_read_lag() {
-  static_assert(kStages == 3, "the immediate below is kStages - 2");
-  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 __device__ __forceinline__ void fence_proxy_async_all() { asm volatile("fence.proxy.async;" ::: "memory"); }
 
@@ -397,6 +383,14 @@ __device__ __forceinline__ float2 leapfrog(float2 kap, float2 nsig, float2 old1,
   return __ffma2_rn(nsig, sneg, __ffma2_rn(kap, d, old2));
 }
 
+// Predicated global store (no branch in the row loop).
+__device__ __forceinline__ void st_global_v4_if(bool p, float* addr, float4 v) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t@q st.global.v4.f32 [%0], {%1, %2, %3, %4};\n\t}" ::"l"(addr),
+      "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(static_cast<uint32_t>(p))
+      : "memory");
+}
+
 // Predicated form: no branch (and no divergence bookkeeping) in the row loop.
 __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, uint32_t bar) {
   asm volatile(
@@ -476,7 +470,7 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
           *reinterpret_cast<float4*>(yc + k * RS) = nw; \
           if (fwd) { \
             if (ADJ) { \
-              *reinterpret_cast<float4*>(stg + k * SW) = make_float4(s_lo.x, s_lo.y, s_hi.x, s_hi.y); \
+              st_global_v4_if(active, stg + k * SW, make_float4(s_lo.x, s_lo.y, s_hi.x, s_hi.y)); \
               acc[k][0] = __ffma2_rn(s_lo, s_lo, acc[k][0]); \
               acc[k][1] = __ffma2_rn(s_hi, s_hi, acc[k][1]); \
             } \
@@ -848,7 +842,9 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
         const float4 h2 = *reinterpret_cast<const float4*>(xc + (H + 2) * RS);
         const float4 h3 = *reinterpret_cast<const float4*>(xc + (H + 3) * RS);
         float* const dstg = S.dummy + (H + 4) * RS;
-        float* stg = (fwd && ADJ) ? (active ? stage_buf(bi) + lr0 * SW + 4 * cg : dstg) : nullptr;
+        // forward of an adjoint mode: -S of this step straight to the band's history slab in HBM
+        float* stg = (fwd && ADJ) ? hist_mine + static_cast<size_t>(lvl - lvl_lo) * hist_step + lr0 * SW + 4 * cg
+                                  : nullptr;
         const float* hl = fwd ? nullptr : (active ? stage_buf(bi) + lr0 * SW + 4 * cg : dstg);
         auto as4 = [](const float2(&r)[2]) { return make_float4(r[0].x, r[0].y, r[1].x, r[1].y); };
         // Threads on the lower band edge compute their bottom rows first, so
@@ -906,13 +902,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
           }
         }
       }
-      if (fwd && ADJ) {
-        fence_proxy_async_smem();
-        if (warp0 && step > 0 && tid == 0) bulk_wait_read_lag();   // the slab to be refilled next step has left shared memory
-      }
       __syncthreads();
-      if (fwd && ADJ && warp0 && tid == 0)
-        bulk_store(hist_mine + static_cast<size_t>(lvl - lvl_lo) * hist_step, smem_u32(stage_buf(bi)), stage_bytes);
       if (!SEG && fwd && rank == rec_rank) {
         // The ring holds the receiver rows [flushed, lvl-1] (level lvl-1 was
         // recorded at this step's start).  A full ring, and at the end every
@@ -983,10 +973,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     if (MODE == SS_MODE_FORWARD) continue;
 
     // ---- forward epilogue: illumination = sum_t (S/12)^2 on model cells --
-    if (tid == 0) {
-      bulk_wait_all();
-      fence_proxy_async_all();
-    }
+    fence_proxy_async_all();   // every thread's history stores, before the adjoint's bulk loads read them
     {
       float* il = P.illum + out_off;
 #pragma unroll
