@@ -383,10 +383,11 @@ __device__ __forceinline__ float2 leapfrog(float2 kap, float2 nsig, float2 old1,
   return __ffma2_rn(nsig, sneg, __ffma2_rn(kap, d, old2));
 }
 
-// Predicated global store (no branch in the row loop).
+// Predicated global store (no branch in the row loop), streaming (.cs): the
+// history is read back only after the whole forward sweep.
 __device__ __forceinline__ void st_global_v4_if(bool p, float* addr, float4 v) {
   asm volatile(
-      "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t@q st.global.v4.f32 [%0], {%1, %2, %3, %4};\n\t}" ::"l"(addr),
+      "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t@q st.global.cs.v4.f32 [%0], {%1, %2, %3, %4};\n\t}" ::"l"(addr),
       "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(static_cast<uint32_t>(p))
       : "memory");
 }
