@@ -51,7 +51,7 @@ constexpr int kMaxThreads = 384;           // register budget: 168 regs/thread
 constexpr int kMaxCluster = 16;
 constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush (at most)
 constexpr int kMinTraceRing = 8;           // the fewest, for grids whose shared memory is tight
-constexpr int kStages = 3;                 // history slabs in flight: prefetch / retire depth kStages-1
+constexpr int kStages = 3;                 // adjoint history slabs in shared memory: prefetch depth kStages-1
 constexpr int kFastRS = 156;               // shared row stride of the 150-column padded OpenFWI grid
 constexpr size_t kMaxSmem = 227 * 1024;
 // The fixed-geometry kernels allocate kCoefCols of an SM's 512 tensor-memory
@@ -250,7 +250,7 @@ struct KParams {
 
 struct Smem {
   float* f[2];
-  float* stg0;     // kStages history slabs of bh x sw, consecutive
+  float* stg0;     // kStages history slabs of bh x sw, consecutive (the adjoint's prefetch ring)
   float* wav;
   float* red;
   float* res0;     // kStages residual rows of nxs, consecutive
