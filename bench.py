@@ -35,7 +35,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -55,7 +54,10 @@ RHOS = (0.6, 1.0, 1.4)
 FLOP_PER_SHOT_IMAGE = 150 * 150 * 1000 * 36
 WORKLOAD = ('RTM images: 500 seeded OpenFWI-shaped synthetic models x 3 backgrounds x 5 shots = 7500 shot-images, '
             '70x70 cells + 40-cell absorbing pad, 1000 steps, one launch')
-CPU_SAMPLE_ROWS = 6          # background rows (x 5 shots) per CPU measurement
+CPU_BEST_ROWS = 12           # background rows (4 models x 3) per CPU call: the CPU path's best batch
+CPU_PROCESS_ROWS = 3         # 2_process's defaults (--batch 1: one model x 3 backgrounds, --threads 2),
+CPU_PROCESS_THREADS = 2      # 2_process.py:115,118
+TRAFFIC_FILE = ROOT / 'profiles' / 'images_kernel_dram.json'
 
 
 def parse():
@@ -173,12 +175,32 @@ def fp32_peak(device):
 
 
 def dram_bytes_per_solve():
-    """Per-solve DRAM traffic of the images kernel from the committed ncu summary, or None."""
-    path = ROOT / 'profiles' / 'images_kernel_70x70.md'
-    if not path.exists():
-        return None
-    m = re.search(r'dram_bytes_per_solve\s*=\s*([0-9.eE+]+)', path.read_text())
-    return float(m.group(1)) if m else None
+    """(bytes, source): DRAM read + write bytes per solve of the images kernel, from one ncu capture of a
+    small case (one round of solves) recorded in a committed data file, or (None, reason)."""
+    try:
+        rec = json.loads(TRAFFIC_FILE.read_text())
+        return float(rec['dram_bytes_per_solve']), rec.get('capture', '')
+    except (OSError, ValueError, KeyError):
+        return None, 'no traffic record'
+
+
+def cpu_model():
+    try:
+        with open('/proc/cpuinfo') as f:
+            for line in f:
+                if line.startswith('model name'):
+                    return line.split(':', 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or 'unknown'
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 def cpu_port_rate(obs_rows, bgs, vm, rows, threads, repeats=3):
@@ -203,14 +225,14 @@ def run_reference(args):
         return 0
     import torch
     from oracle import oracle as O
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     torch.set_num_threads(threads)
-    models = population_slice(0, 2, N_MODELS)
+    rows = CPU_BEST_ROWS
+    models = population_slice(0, rows // len(RHOS), N_MODELS)
     trend = depth_trend(population_slice(0, N_MODELS, N_MODELS))
     bgs, vm = backgrounds_for(models, trend)
     osim = O.OracleSim(dtype=torch.float32)
     obs = np.repeat(osim.gathers(models.astype(np.float64)), len(RHOS), 0)
-    rows = CPU_SAMPLE_ROWS
     for _ in range(args.warmup):
         osim.images(bgs[:rows], obs[:rows], v_mute=vm[:rows])
     t0 = time.perf_counter()
@@ -218,14 +240,16 @@ def run_reference(args):
         osim.images(bgs[:rows], obs[:rows], v_mute=vm[:rows])
     elapsed = time.perf_counter() - t0
     value = rows * 5 * args.steps / elapsed
-    sample = (f'{rows} background rows x 5 shots = {rows * 5} shot-images per step from the same workload, '
-              f'float32 PyTorch eager on {threads} host threads')
+    sample = (f'{rows} background rows (the first {rows // len(RHOS)} models x 3 backgrounds) x 5 shots = '
+              f'{rows * 5} shot-images per step from the same workload, float32 PyTorch eager on {threads} host '
+              f'threads ({cpu_model()})')
     print(json.dumps({
         'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus,
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': elapsed / args.steps * 1e3,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
         'config': {'workload': WORKLOAD, 'sample': sample},
-        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': threads, 'kind': 'port', 'sample': sample},
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': threads, 'kind': 'port', 'sample': sample,
+                         'cpu_model': cpu_model()},
         'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }), flush=True)
     return 0
@@ -305,31 +329,62 @@ def run_ours(args):
     h2d = obs_host.numel() * 4 + bgs.size * 8 + vm.size * 8
     d2h = img.numel() * 4 * 2
     sim.images(bgs, obs_host, v_mute=vm)
+    e2e_steps = max(1, min(args.steps, 10))
     D.barrier()
     t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 3))
     for _ in range(e2e_steps):
         sim.images(bgs, obs_host, v_mute=vm)
     e2e_s = D.reduce(time.perf_counter() - t0, 'max', dev if world > 1 else None)
     e2e = world * shot_images * e2e_steps / e2e_s
+    # the same call with pageable NumPy gathers (what the reference's callers pass)
+    obs_np = obs_host.numpy().copy()
+    del obs_host
+    D.barrier()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        sim.images(bgs, obs_np, v_mute=vm)
+    e2e_np = world * shot_images * 2 / D.reduce(time.perf_counter() - t0, 'max', dev if world > 1 else None)
+    # driven as 2_process drives it (2_process.py:166-204): models in batches of
+    # budget // imaging_memory_bytes(3) at the default 2 GiB, float64 NumPy gathers repeated per background
+    per_call = int(2.0 * 1024 ** 3 // gpu.imaging_memory_bytes(len(RHOS)))
+    obs_models = obs_np[::len(RHOS)].astype(np.float64)
+    del obs_np
+    D.barrier()
+    t0 = time.perf_counter()
+    for i in range(0, per, per_call):
+        j = min(per, i + per_call)
+        sim.images(bgs[i * len(RHOS):j * len(RHOS)], np.repeat(obs_models[i:j], len(RHOS), 0),
+                   v_mute=vm[i * len(RHOS):j * len(RHOS)])
+    e2e_proc = world * shot_images / D.reduce(time.perf_counter() - t0, 'max', dev if world > 1 else None)
+    del obs_models
 
     peak = fp32_peak(dev)
     achieved = FLOP_PER_SHOT_IMAGE * shot_images / (launch_ms * 1e-3) / 1e12
-    per_solve = dram_bytes_per_solve()
+    per_solve, traffic_src = dram_bytes_per_solve()
     roofline = {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
                 'traffic': per_solve * shot_images if per_solve else None,
                 'peak_source': 'measured live: max of scalar FFMA and packed FFMA2 probes on all SMs '
                                '(MEASURED_PEAKS.json has no FP32 figure)',
                 'algorithmic': '36 flops per padded cell per step (16 forward + 20 adjoint), 150^2 cells, 1000 steps; '
-                               'traffic = ncu dram bytes per solve (profiles/images_kernel_70x70.md) x solves'}
+                               'traffic = ncu dram read + write bytes per solve x solves',
+                'traffic_source': traffic_src,
+                'hbm_gbs_of_traffic': per_solve * shot_images / (launch_ms * 1e-3) / 1e9 if per_solve else None}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        obs_rows = obs[:CPU_SAMPLE_ROWS].cpu().double().numpy()
-        rate = cpu_port_rate(obs_rows, bgs, vm, CPU_SAMPLE_ROWS, threads)
-        cpu = {'value': rate, 'unit': UNIT, 'cores': threads, 'kind': 'port',
-               'sample': f'{CPU_SAMPLE_ROWS} background rows x 5 shots of the same workload (median of 3), '
-                         f'oracle float32 PyTorch-eager restatement of Sim.images on {threads} threads'}
+        import torch as _t
+        threads = host_threads()
+        rows = CPU_BEST_ROWS
+        obs_rows = obs[:rows].cpu().double().numpy()
+        rate = cpu_port_rate(obs_rows, bgs, vm, rows, threads)
+        rate_proc = cpu_port_rate(obs_rows, bgs, vm, CPU_PROCESS_ROWS, CPU_PROCESS_THREADS)
+        _t.set_num_threads(threads)
+        cpu = {'value': rate, 'unit': UNIT, 'cores': threads, 'kind': 'port', 'cpu_model': cpu_model(),
+               'sample': f'{rows} background rows (4 models x 3 backgrounds) x 5 shots of the same workload, median '
+                         f'of 3 calls: the oracle\'s float32 PyTorch-eager restatement of Sim.images on {threads} '
+                         f'host threads',
+               'process_defaults': {'value': rate_proc, 'unit': UNIT, 'cores': CPU_PROCESS_THREADS,
+                                    'sample': f'{CPU_PROCESS_ROWS} background rows (one model, 2_process --batch 1) '
+                                              f'on {CPU_PROCESS_THREADS} threads (2_process --threads 2)'}}
     if rank == 0:
         print(json.dumps({
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
@@ -343,7 +398,14 @@ def run_ours(args):
                        'cuda_graph': captured, 'plan': eng.plan(n_rows, 2)},
             'roofline': roofline, 'cpu_baseline': cpu,
             'e2e': {'value': e2e, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
-                    'api': 'shotsweep_b200.gpu.Sim.images (pinned torch gathers, numpy velocities in; numpy out)'},
+                    'api': 'shotsweep_b200.gpu.Sim.images (pinned torch gathers, numpy velocities in; numpy out)',
+                    'steps': e2e_steps,
+                    'numpy_pageable': {'value': e2e_np, 'unit': UNIT,
+                                       'api': 'Sim.images with pageable float32 NumPy gathers (staged per chunk)'},
+                    'process_batches': {'value': e2e_proc, 'unit': UNIT, 'models_per_call': per_call,
+                                        'api': 'Sim.images on budget // imaging_memory_bytes(3) models per call at '
+                                               '2 GiB, float64 NumPy gathers repeated per background, as '
+                                               '2_process.py:166-204'}},
             'clocks': clocks, 'gpu_launches': args.steps,
         }), flush=True)
     del graph

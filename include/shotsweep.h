@@ -8,7 +8,7 @@
  * The reference is pure Python (openfwi/physics/gpu.py); it has no FFI.  Each
  * entry point below replaces the computational core of one method of the
  * reference's `Sim` class or one module-level helper, and is what a ctypes
- * binding of that method calls (see INTEGRATION.md for the binding).
+ * binding of that method calls (shotsweep_b200/_lib.py is that binding).
  *
  * Conventions
  *   - All array pointers are DEVICE pointers, C-contiguous float32 unless the
@@ -44,7 +44,7 @@ typedef enum ss_status {
     SS_ERR_UNSUPPORTED = -2,  /* geometry does not fit any kernel plan         */
     SS_ERR_CUDA = -3,         /* a CUDA runtime call failed                    */
     SS_ERR_TIMEOUT = -4,      /* a device-side bounded wait ran out            */
-    SS_ERR_WORKSPACE = -5,    /* workspace missing or smaller than required    */
+    SS_ERR_WORKSPACE = -5,    /* workspace missing or too small for one solve  */
     SS_ERR_NONFINITE = -6     /* observed gathers hold NaN or infinity         */
 } ss_status;
 
@@ -79,8 +79,19 @@ const char* ss_version(void);
 const char* ss_last_error(void);
 
 /* Bytes of device workspace that a call with this geometry, number of
- * velocity models and mode needs on the current device. */
+ * velocity models and mode needs on the current device to keep every
+ * co-resident cluster busy.  ss_gradient / ss_images accept a smaller
+ * workspace and then keep fewer solves in flight (as many as it holds; at
+ * least one).  Memory model of the reference: imaging_memory_bytes
+ * (openfwi/physics/gpu.py:70-73). */
 size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mode);
+
+/* Bytes of workspace for a call that keeps at most `slots` solves in flight
+ * (per-solve scratch: the per-step history of one solve and its trace,
+ * padded-gradient and gradient rows).  Needs no device: a caller with a
+ * memory budget sizes its workspace with it before any launch.  Used by the
+ * drop-in's imaging_memory_bytes (openfwi/physics/gpu.py:70-73). */
+size_t ss_workspace_bytes_slots(const ss_geometry* geom, int32_t mode, int32_t slots);
 
 /* Reads the device-side status word of `workspace` after synchronising
  * `stream`: SS_OK, SS_ERR_TIMEOUT if a bounded wait ran out, or

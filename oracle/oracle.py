@@ -281,3 +281,19 @@ def depth_trend(models):
     """Mean over models of mean_x v(z) - mean_x v(0) (openfwi/physics/background.py:91-94)."""
     m = np.asarray(models, np.float64)
     return (m.mean(2) - m[:, :1, :].mean(2)).mean(0)
+
+
+def calibrate(models, gathers, eps=1e-3, dtype=torch.float32, geom=Geometry()):
+    """Pooled frequency-domain Wiener estimate of the effective source wavelet (gpu.py:213-221).
+
+    The reference simulates the known models with the Ricker in its default
+    float32 (``Sim(RICKER)``, gpu.py:215), then shapes the Ricker by the
+    cross-spectrum of synthetics and observations over their power spectrum,
+    both summed over models, shots and receivers, regularised by eps x the
+    power spectrum's peak."""
+    sims = OracleSim(ricker(geom.nt, geom.dt), dtype=dtype, geom=geom).gathers(np.asarray(models, np.float64))
+    sf = np.fft.rfft(sims, axis=2)
+    of = np.fft.rfft(np.asarray(gathers, np.float64), axis=2)
+    num = (np.conj(sf) * of).sum(axis=(0, 1, 3))
+    den = (np.abs(sf) ** 2).sum(axis=(0, 1, 3))
+    return np.fft.irfft(np.fft.rfft(ricker(geom.nt, geom.dt)) * num / (den + eps * den.max()), n=geom.nt)

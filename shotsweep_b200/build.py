@@ -29,7 +29,7 @@ def nvcc():
 
 
 def command(output=LIBRARY, verbose=False, extra=()):
-    cmd = [nvcc(), *ARCH, '-O3', '-lineinfo', '-std=c++17', '--use_fast_math' if False else '-ftz=false',
+    cmd = [nvcc(), *ARCH, '-O3', '-lineinfo', '-std=c++17', '-ftz=false',
            '-Xcompiler', '-fPIC', '-shared', f'-I{ROOT / "include"}', '-o', str(output),
            *[str(s) for s in SOURCES], '-lcudart', *extra]
     if verbose:

@@ -1365,7 +1365,9 @@ size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring) {
          (kStages + 3) * sizeof(uint64_t);   // barriers, then the TMEM address word
 }
 
-int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
+// The band plan of a geometry: cluster size, band height, threads and shared
+// memory (arithmetic only; make_plan adds what the device can hold at once).
+int plan_shape(const ss_geometry* g, int mode, Plan* p) {
   constexpr int H = kRowsPerThread;
   const bool adj = mode != SS_MODE_FORWARD;
   p->nzp = g->nz + 2 * g->pad;
@@ -1400,6 +1402,14 @@ int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
   p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
   p->smem = std::max(p->smem, kTcMinSmem);
   p->fast = fast_geometry(g->nx, g->pad);
+  p->max_clusters = 0;
+  p->slots = 1;
+  return SS_OK;
+}
+
+int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
+  int rc = plan_shape(g, mode, p);
+  if (rc) return rc;
   const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->fast));
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->smem));
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
@@ -1451,6 +1461,20 @@ WsLayout ws_layout(const ss_geometry* g, const Plan& p, int mode, int hist_steps
   }
   w.total = off;
   return w;
+}
+
+// The most solves in flight whose scratch fits `bytes` (0: not even one).
+int slots_for_bytes(const ss_geometry* g, Plan p, int mode, size_t bytes) {
+  p.slots = 1;
+  if (ws_layout(g, p, mode).total > bytes) return 0;
+  const size_t one = ws_layout(g, p, mode).total;
+  p.slots = 2;
+  const size_t per_slot = ws_layout(g, p, mode).total - one;   // alignment padding included
+  if (per_slot == 0) return 1 << 30;                          // forward mode: no per-slot scratch
+  int n = static_cast<int>(std::min<size_t>((bytes - one) / per_slot + 1, size_t(1) << 30));
+  p.slots = n;
+  while (n > 1 && ws_layout(g, p, mode).total > bytes) p.slots = --n;
+  return n;
 }
 
 KParams base_params(const ss_geometry* g, const Plan& p, int n_models) {
@@ -1517,8 +1541,10 @@ int run_adjoint(int mode, const ss_geometry* g, int n_models, const float* vel, 
   Plan p;
   rc = make_plan(g, mode, n_models * g->n_shots, &p);
   if (rc) return rc;
+  // A workspace smaller than the full plan's keeps fewer solves in flight.
+  p.slots = std::min(p.slots, slots_for_bytes(g, p, mode, ws ? ws_bytes : 0));
+  if (p.slots < 1) return fail(SS_ERR_WORKSPACE, "workspace missing or too small for one solve in flight");
   const WsLayout L = ws_layout(g, p, mode);
-  if (!ws || ws_bytes < L.total) return fail(SS_ERR_WORKSPACE, "workspace missing or too small");
   unsigned char* w = static_cast<unsigned char*>(ws);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   SS_CUDA(cudaMemsetAsync(w + L.err, 0, 256, st));
@@ -2063,6 +2089,14 @@ size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mod
   if (check_geometry(geom) || n_models < 1 || mode < 0 || mode > 2) return 0;
   Plan p;
   if (make_plan(geom, mode, n_models * geom->n_shots, &p)) return 0;
+  return ws_layout(geom, p, mode).total;
+}
+
+size_t ss_workspace_bytes_slots(const ss_geometry* geom, int32_t mode, int32_t slots) {
+  if (check_geometry(geom) || slots < 1 || mode < 0 || mode > 2) return 0;
+  Plan p;
+  if (plan_shape(geom, mode, &p)) return 0;
+  p.slots = slots;
   return ws_layout(geom, p, mode).total;
 }
 

@@ -5,7 +5,9 @@ grid / time axis / shot layout that the kernels plan for (the reference's
 ``Sim`` hard-wires 70x70, 1000 steps, 5 shots; ``shotsweep_b200.gpu.Sim`` is a
 thin layer over this class with that geometry).  Arguments are CUDA float32
 tensors; outputs are new CUDA tensors.  The per-step history workspace is
-allocated once and reused while it is large enough.
+allocated once and reused while it is large enough.  ``max_slots`` caps the
+solves in flight (each holds its own history, about 89 MB for the OpenFWI
+grid), which bounds the workspace of a call.
 """
 from __future__ import annotations
 
@@ -32,6 +34,7 @@ class Engine:
             self.device = torch.device('cuda', torch.cuda.current_device())
         self.L = _lib.load()
         self._ws = None
+        self.max_slots = None     # None: every co-resident cluster gets a solve
 
     # -- plumbing -----------------------------------------------------------
     @property
@@ -51,17 +54,26 @@ class Engine:
         with torch.cuda.device(self.device):
             _lib.check(self.L.ss_plan_info(ctypes.byref(self.g), n_models, mode, out), 'ss_plan_info')
         keys = ('cluster', 'threads', 'smem', 'band_rows', 'col_groups', 'rows_per_thread', 'max_clusters', 'slots')
-        return dict(zip(keys, list(out)))
+        info = dict(zip(keys, list(out)))
+        if self.max_slots is not None and mode != _lib.MODE_FORWARD:
+            info['slots'] = max(1, min(info['slots'], int(self.max_slots)))
+        return info
 
     def workspace(self, n_models, mode):
+        """The workspace of a call: a view of the engine's buffer, exactly as long as the call's plan needs
+        (the library keeps as many solves in flight as the workspace it is given holds)."""
         with torch.cuda.device(self.device):
-            need = self.L.ss_workspace_bytes(ctypes.byref(self.g), n_models, mode)
+            if self.max_slots is not None and mode != _lib.MODE_FORWARD:
+                slots = self.plan(n_models, mode)['slots']
+                need = self.L.ss_workspace_bytes_slots(ctypes.byref(self.g), mode, slots)
+            else:
+                need = self.L.ss_workspace_bytes(ctypes.byref(self.g), n_models, mode)
         if need == 0:
             _lib.check(_lib.ERR_UNSUPPORTED, 'ss_workspace_bytes')
         if self._ws is None or self._ws.numel() < need:
             self._ws = None
             self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
-        return self._ws
+        return self._ws[:need]
 
     def _stream(self):
         return _lib.stream_handle(self.device)
@@ -148,14 +160,16 @@ class Engine:
         is small, so that little is left to copy back at the end: a call costs about the imaging time.
         vel: [B, nz, nx], float32 on the device, or float32 / float64 on the host (each chunk's rows are
         converted into a pinned float32 buffer just before its copy, while the previous chunk is imaged).
-        obs_host: CPU tensor [B, S, nt, nx] float32, pinned or not (pageable rows are staged through pinned
-        buffers).  `chunk_rows` fixes a uniform chunk size instead.
+        obs_host: CPU tensor [B, S, nt, nx], float32 (pinned or not) or float64; pageable or float64 rows are
+        staged (and converted) through pinned float32 buffers chunk by chunk, while the previous chunk is
+        imaged.  `chunk_rows` fixes a uniform chunk size instead.
         """
         g = self.g
         B = vel.shape[0]
         shape = (B, g.n_shots, g.nt, g.nx)
-        if not isinstance(obs_host, torch.Tensor) or obs_host.device.type != 'cpu' or obs_host.dtype != torch.float32:
-            raise ValueError('obs_host must be a float32 CPU tensor')
+        if (not isinstance(obs_host, torch.Tensor) or obs_host.device.type != 'cpu'
+                or obs_host.dtype not in (torch.float32, torch.float64)):
+            raise ValueError('obs_host must be a float32 or float64 CPU tensor')
         if tuple(obs_host.shape) != shape:
             raise ValueError(f'obs must have shape {shape}, got {tuple(obs_host.shape)}')
         obs_host = obs_host.contiguous()
@@ -178,7 +192,7 @@ class Engine:
         h2d, d2h = self._copy_streams
         h2d.wait_stream(compute)          # inputs and outputs made on the caller's stream are ready
         dev_obs = [torch.empty(chunk, *shape[1:], **f32) for _ in range(min(2, n_chunks))]
-        pinned = obs_host.is_pinned()
+        pinned = obs_host.dtype == torch.float32 and obs_host.is_pinned()
         staging = [] if pinned else [torch.empty(chunk, *shape[1:], dtype=torch.float32, pin_memory=True)
                                      for _ in range(min(2, n_chunks))]
         vel_staging = [torch.empty(chunk, g.nz, g.nx, dtype=torch.float32, pin_memory=True)

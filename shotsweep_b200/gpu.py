@@ -14,9 +14,15 @@ Differences a caller can observe:
     dictionary: the adjoint keeps a full per-step history in device memory
     instead of recomputing segments, so its results do not depend on it (the
     reference's own test pins that invariance, tests/test_physics.py:76-79).
-  * ``imaging_memory_bytes`` reports this implementation's device storage.
+  * ``imaging_memory_bytes`` reports this implementation's device storage,
+    and ``images`` / ``gradient`` keep their storage within it by running at
+    most rows*5/SOLVES_PER_SLOT solves at once (a call on 90 or more rows,
+    30 models at 3 backgrounds, fills the 45 co-resident clusters of a B200).
 """
 from __future__ import annotations
+
+import contextlib
+import math
 
 import numpy as np
 import torch
@@ -84,19 +90,45 @@ def fold_edge_padding(g, pad):
                       (batch, nz, nx, pad))
 
 
-def imaging_memory_bytes(batch, pad=40, checkpoint_interval=40, bytes_per_value=4):
-    """Device storage of one imaging call on ``batch`` background rows.
+# A call on B background rows (5 solves each) keeps at most B*5 / SOLVES_PER_SLOT
+# solves in flight (at least one), so that its scratch grows with the call
+# like the reference's per-row checkpoint storage does.
+SOLVES_PER_SLOT = 10
 
-    The reference models its own checkpoint storage (gpu.py:70-73).  Here the
-    per-row tensors are the observed gathers, outputs and velocity; the
-    per-step history lives in a workspace shared by the solves in flight (at
-    most one per co-resident cluster), so it does not grow with ``batch``.
+
+def _slot_bytes(pad):
+    """(workspace with one solve in flight, bytes per further solve) for the OpenFWI grid: per-step history,
+    trace, gradient rows."""
+    L = _lib.load()
+    g = engine.geometry(NZ, NX, NT, pad, SRC)
+    one = L.ss_workspace_bytes_slots(g, _lib.MODE_IMAGES, 1)
+    two = L.ss_workspace_bytes_slots(g, _lib.MODE_IMAGES, 2)
+    if one == 0 or two == 0:
+        _lib.check(_lib.ERR_UNSUPPORTED, 'ss_workspace_bytes_slots')
+    return one, two - one
+
+
+def max_solves_in_flight(batch):
+    """Solves a call on `batch` background rows keeps in flight (Sim.images / Sim.gradient)."""
+    return max(1, (int(batch) * len(SRC)) // SOLVES_PER_SLOT)
+
+
+def imaging_memory_bytes(batch, pad=40, checkpoint_interval=40, bytes_per_value=4):
+    """Device storage of one Sim.images / Sim.gradient call on ``batch`` background rows (gpu.py:70-73).
+
+    Linear in ``batch`` like the reference's model, so that a caller's
+    ``budget // imaging_memory_bytes(rows)`` (2_process.py:166-171) bounds the
+    real use: per row, the gathers, outputs and velocity copies on the device,
+    plus 1/SOLVES_PER_SLOT of one solve's scratch per solve, because the call
+    keeps at most rows*5/SOLVES_PER_SLOT solves (their per-step histories) in
+    flight.  A single row still needs one solve's scratch, hence the floor.
+    ``checkpoint_interval`` does not apply: the adjoint reads a full history.
     """
-    n = NZ + 2 * pad
-    rows = batch * 5 * bytes_per_value * (NT * NX + 3 * NZ * NX) + batch * NZ * NX * bytes_per_value
-    in_flight = min(batch * 5, 74)          # one solve per 2-SM cluster on a 148-SM B200
-    history = in_flight * bytes_per_value * (NT * (n * n + NX) + 2 * n * n)
-    return int(rows + history)
+    one_slot, per_slot = _slot_bytes(pad)
+    scale = bytes_per_value / 4.0
+    row = len(SRC) * (NT * NX + 2 * NZ * NX) * bytes_per_value + NZ * NX * bytes_per_value
+    linear = batch * (row + len(SRC) * per_slot * scale / SOLVES_PER_SLOT)
+    return int(math.ceil(max(linear, batch * row + one_slot * scale)))
 
 
 class Sim:
@@ -161,6 +193,16 @@ class Sim:
             raise ValueError(f'observations must be finite with shape {(B, 5, NT, NX)}')
         return observed
 
+    @contextlib.contextmanager
+    def _in_flight(self, B):
+        """Cap the solves in flight of one call on B rows (imaging_memory_bytes' storage model)."""
+        eng = self.engine
+        eng.max_slots = max_solves_in_flight(B)
+        try:
+            yield
+        finally:
+            eng.max_slots = None
+
     def _finish(self, B):
         try:
             self.engine.status()
@@ -200,9 +242,10 @@ class Sim:
         """Per-shot gradient and illumination as device tensors (gpu.py:152-188)."""
         v = self._velocity(v_bg)
         B = len(v)
-        grad, illum = self.engine.gradient(self._to_dev(v), self._wavelet(), self._observed(obs, B),
-                                           self._mute(v_mute, B), t_mute)
-        self._finish(B)
+        with self._in_flight(B):
+            grad, illum = self.engine.gradient(self._to_dev(v), self._wavelet(), self._observed(obs, B),
+                                               self._mute(v_mute, B), t_mute)
+            self._finish(B)
         return grad, illum
 
     @torch.no_grad()
@@ -222,10 +265,16 @@ class Sim:
             raise ValueError('illumination regularization eps must be positive')
         v = self._velocity(v_bg)
         B = len(v)
+        with self._in_flight(B):
+            return self._images(v, obs, v_mute, t_mute, eps, laplacian)
+
+    def _images(self, v, obs, v_mute, t_mute, eps, laplacian):
+        B = len(v)
         host = not (isinstance(obs, torch.Tensor) and obs.is_cuda)
         if host:   # host observations: copies overlapped with imaging, chunk by chunk
             o = obs if isinstance(obs, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(obs))
-            o = o.to(torch.float32) if o.dtype != torch.float32 else o
+            if o.dtype not in (torch.float32, torch.float64):   # float64 rows convert chunk by chunk
+                o = o.to(torch.float32)
             if tuple(o.shape) != (B, 5, NT, NX):                                   # gpu.py:156-157
                 raise ValueError(f'observations must be finite with shape {(B, 5, NT, NX)}')
             try:   # float64 model rows are converted and copied chunk by chunk

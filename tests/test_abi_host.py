@@ -96,10 +96,46 @@ def test_velocity_validation_happens_on_host():
 
 
 def test_memory_model_is_bounded():
+    """The reference's own bound (tests/test_physics.py:81-83), and a model linear in the rows."""
     from shotsweep_b200 import gpu
     full_history = 24 * 5 * 1000 * 150 * 150 * 4
-    assert gpu.imaging_memory_bytes(24) < full_history         # history is shared by solves in flight
+    assert gpu.imaging_memory_bytes(24) < full_history / 5
     assert gpu.imaging_memory_bytes(1) < gpu.imaging_memory_bytes(300)
+    for rows in (3, 6, 30, 300):
+        assert abs(gpu.imaging_memory_bytes(2 * rows) - 2 * gpu.imaging_memory_bytes(rows)) <= 2
+
+
+def test_process_budget_formula_batches_many_models():
+    """2_process.py:166-171 sizes its batch as budget // imaging_memory_bytes(3 rows): at the default 2 GiB
+    that admits at least 15 models, and the scratch of a call on that batch (at most rows*5/10 solves in
+    flight, each with its own history) stays inside the budget with the call's row tensors."""
+    import ctypes
+    from shotsweep_b200 import _lib, engine, gpu
+    L = _lib.load()
+    per_model = gpu.imaging_memory_bytes(3)
+    max_batch = int(2.0 * 1024 ** 3 // per_model)
+    assert max_batch >= 15
+    rows = 3 * max_batch
+    slots = gpu.max_solves_in_flight(rows)
+    g = engine.geometry()
+    ws = L.ss_workspace_bytes_slots(ctypes.byref(g), _lib.MODE_IMAGES, slots)
+    row_tensors = rows * (5 * (1000 * 70 + 2 * 70 * 70) + 70 * 70) * 4
+    assert ws + row_tensors <= max_batch * per_model <= 2.0 * 1024 ** 3
+    assert 20 <= slots <= 45
+
+
+def test_workspace_per_slot_is_linear(lib):
+    """ss_workspace_bytes_slots needs no device and grows by one solve's scratch per slot."""
+    import ctypes
+    from shotsweep_b200 import _lib, engine
+    g = engine.geometry()
+    sizes = [lib.ss_workspace_bytes_slots(ctypes.byref(g), _lib.MODE_IMAGES, k) for k in (1, 2, 3, 45)]
+    step = sizes[1] - sizes[0]
+    assert abs(sizes[2] - sizes[1] - step) <= 1024 and abs(sizes[3] - sizes[0] - 44 * step) <= 44 * 1024
+    assert sizes == sorted(sizes)                  # (regions are 256-byte aligned, so steps differ by bytes)
+    assert 88e6 < step < 90e6                      # 1000 steps x 150 rows x 148 columns x 4 bytes, + rows
+    assert lib.ss_workspace_bytes_slots(ctypes.byref(g), _lib.MODE_IMAGES, 0) == 0
+    assert lib.ss_workspace_bytes_slots(ctypes.byref(g), _lib.MODE_FORWARD, 45) == 256
 
 
 def test_host_pipeline_chunks_cover_rows_in_whole_rounds():

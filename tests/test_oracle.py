@@ -118,3 +118,29 @@ def test_image_cache_oracle_is_the_reference_epilogue():
     assert scale[0] == np.percentile(a.reshape(1, -1), 99, axis=1)[0]
     with pytest.raises(ValueError):
         PP.image_cache(np.zeros_like(img))
+
+
+def test_oracle_calibrate_matches_reference():
+    """calibrate() restated (gpu.py:213-221): float32 synthetics, pooled Wiener shaping of the Ricker."""
+    c = golden('calib_small')
+    torch.set_num_threads(max(1, torch.get_num_threads()))
+    wavelet = O.calibrate(c['models'], c['observed'].astype(np.float64))
+    assert rel(wavelet, c['wavelet']) < 1e-6
+
+
+def test_oracle_finite_difference_matches_reference_top_strip():
+    """The float64 oracle's loss gives the reference's own central difference along the top strip (the
+    direction that edge padding folds onto the source row; tests/test_physics.py:48), epsilon 0.1 m/s."""
+    fx = golden('fd_directions')
+    velocity, observed = fx['velocity'], fx['observed'].astype(np.float64)
+    eps = float(fx['epsilon'])
+    sim = O.OracleSim()
+    d = np.zeros_like(velocity)
+    d[0, 0, 25:45] = 1.0
+
+    def loss(v):
+        r = sim.gathers(v) - observed
+        return 0.5 * np.sum(r * r)
+
+    fd = (loss(velocity + eps * d) - loss(velocity - eps * d)) / (2 * eps)
+    assert abs(fd - float(fx['fd_top_boundary'])) <= 1e-8 * abs(fd)

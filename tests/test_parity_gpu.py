@@ -85,6 +85,58 @@ def test_module_helpers_match_reference(gpu):
     np.testing.assert_allclose(mute, g['mute_sub'], rtol=0, atol=2e-6)
 
 
+CALIBRATE_TOL = 1e-5
+
+
+def test_calibrate_matches_reference(gpu):
+    """Source calibration (gpu.py:213-221) against the reference's own output on two seeded models whose
+    observed gathers carry a phase-rotated, delayed, scaled Ricker (tests/golden/calib_small.npz): the
+    drop-in's forward modelling runs on the GPU, the pooled Wiener filter on the host."""
+    c = golden('calib_small')
+    wavelet = gpu.calibrate(list(c['models']), list(c['observed'].astype(np.float64)))
+    assert wavelet.shape == c['wavelet'].shape and np.isfinite(wavelet).all()
+    assert rel(wavelet, c['wavelet']) <= CALIBRATE_TOL
+    # the estimate recovers the shaped source it was given (a property of the method, not only of the code)
+    assert rel(wavelet, c['shaped']) <= 0.05
+
+
+def test_process_batch_stays_within_memory_budget(gpu):
+    """2_process sizes its batch as budget // imaging_memory_bytes(3 rows) (2_process.py:166-171).  A call on
+    that many models, with NumPy gathers as 2_process passes them, allocates no more device memory than the
+    model says (and so stays inside the default 2 GiB), and its images equal those of a call that keeps
+    every co-resident cluster busy, bit for bit (each solve's arithmetic does not depend on its slot)."""
+    from oracle import oracle as O
+    from shotsweep_b200 import engine, synth
+    budget = 2 * 1024 ** 3
+    per_model = gpu.imaging_memory_bytes(3)
+    n = int(budget // per_model)
+    assert n >= 15
+    models = synth.population(n).astype(np.float64)
+    sim = gpu.Sim()
+    obs = sim.gathers(models)
+    trend = O.depth_trend(models)
+    v_s = models[:, 0, :].mean(1)
+    bgs = np.concatenate([O.backgrounds(v, trend) for v in v_s])
+    obs_rows = np.repeat(obs, 3, 0)
+    vm = np.repeat(v_s, 3)
+    torch.cuda.synchronize()
+    fresh = gpu.Sim()
+    base = torch.cuda.memory_allocated()
+    torch.cuda.reset_peak_memory_stats()
+    img, illum = fresh.images(bgs, obs_rows, v_mute=vm)
+    torch.cuda.synchronize()
+    used = torch.cuda.max_memory_allocated() - base
+    assert used <= n * per_model <= budget, (used, n * per_model)
+    eng = fresh.engine
+    assert eng.max_slots is None            # the cap applies to the call only
+    dev = eng.device
+    f32 = dict(dtype=torch.float32, device=dev)
+    ref_img, ref_illum = eng.images(torch.tensor(bgs, **f32), engine.scaled_wavelet(gpu.RICKER, dev),
+                                    torch.tensor(obs_rows, **f32), torch.tensor(vm, **f32))
+    eng.status()
+    assert np.array_equal(img, ref_img.cpu().numpy()) and np.array_equal(illum, ref_illum.cpu().numpy())
+
+
 def test_forward_returns_reference_structures(gpu, plain):
     sim = gpu.Sim(checkpoint_interval=250)
     out, ck, c2 = sim.forward(plain['model'][None], store=True)
