@@ -106,6 +106,14 @@ int32_t ss_workspace_status(const void* workspace, void* stream);
  * in flight for n_models. */
 int32_t ss_plan_info(const ss_geometry* geom, int32_t n_models, int32_t mode, int64_t out[8]);
 
+/* Tile height (rows of its band each thread keeps in registers, 4 or 5) of
+ * the plans of `mode` made after this call, process-wide; 0 restores the
+ * default (5).  Taller tiles reuse more vertical neighbours from registers,
+ * shorter ones allow more threads (warps) per CTA; a tuner times both and
+ * sets the faster.  Every tile height computes the same values.  No
+ * counterpart in the reference (its tensors have no tiles). */
+int32_t ss_set_rows_per_thread(int32_t mode, int32_t rows);
+
 /* Forward modelling.  Replaces Sim.forward / Sim.gathers (gpu.py:117-140).
  *   vel      [n_models, nz, nx]                    velocities (m/s)
  *   wavelet  [nt]                                  scaled source samples
@@ -253,10 +261,14 @@ int32_t ss_wait_probe(int32_t* status, double limit_ms, void* stream);
  * SMs (falls back to 1 when the classes do not split).
  *
  * 1. ss_batch_plan (host): validates the items, forms the classes and the
- *    per-class launch shapes (cluster size from `cluster_by_class`, indexed by
- *    a class's smallest cluster, 0 or NULL = that smallest cluster; an
- *    autotuner fills it), and writes a self-contained plan of *plan_bytes
- *    bytes into `plan` (host memory; NULL: only report the sizes).
+ *    per-class launch shapes, and writes a self-contained plan of
+ *    *plan_bytes bytes into `plan` (host memory; NULL: only report the
+ *    sizes).  `cluster_by_class` (NULL, or SS_MAX_CLUSTER + 1 entries indexed
+ *    by a class's smallest cluster at 5 rows per thread; an autotuner fills
+ *    it) gives each size class its launch shape: bits 0-7 the cluster size
+ *    (0 = that smallest cluster), bits 8-15 the tile height in rows per
+ *    thread, 4..6 (0 = 5).  A solve that does not fit the chosen shape runs
+ *    at the next cluster size that fits it.
  * 2. The caller copies the plan bytes unchanged to device memory.
  * 3. ss_batch_run (stream-ordered): runs every class; the same plan serves
  *    any number of runs with new data in the same layout. */
@@ -286,7 +298,7 @@ typedef struct ss_batch_class_info {
     int32_t smem_bytes;   /* per CTA                                             */
     int32_t slots;        /* persistent clusters launched                        */
     int32_t stream;       /* 0: the caller's stream, 1: the library's second one */
-    int32_t reserved;
+    int32_t rows_per_thread;  /* tile height of the class's launch               */
     double cell_steps;    /* sum over its solves of padded cells x steps         */
 } ss_batch_class_info;
 
@@ -296,6 +308,9 @@ int32_t ss_batch_plan(const ss_physics* phys, int32_t mode, const ss_batch_item*
 /* Smallest cluster (CTAs per solve) that fits the item in `mode`: its size
  * class; negative ss_status if none does. */
 int32_t ss_batch_min_cluster(const ss_batch_item* item, int32_t mode);
+/* The same at `rows` rows per thread (4..6): what an autotuner that picks a
+ * class's tile height needs to know about each of its grids. */
+int32_t ss_batch_min_cluster_rows(const ss_batch_item* item, int32_t mode, int32_t rows);
 int32_t ss_batch_classes(const void* plan, ss_batch_class_info* out, int32_t max_classes, int32_t* n_classes);
 /* wavelet: at least the batch's largest nt samples (scaled as for ss_forward).
  * gathers: forward mode output; img: images mode output; grad: gradient mode

@@ -59,7 +59,7 @@ class BatchClassInfo(ctypes.Structure):
     """Mirror of ss_batch_class_info."""
     _fields_ = [('min_cluster', ctypes.c_int32), ('cluster', ctypes.c_int32), ('n_solves', ctypes.c_int32),
                 ('threads', ctypes.c_int32), ('smem_bytes', ctypes.c_int32), ('slots', ctypes.c_int32),
-                ('stream', ctypes.c_int32), ('reserved', ctypes.c_int32), ('cell_steps', ctypes.c_double)]
+                ('stream', ctypes.c_int32), ('rows_per_thread', ctypes.c_int32), ('cell_steps', ctypes.c_double)]
 
 
 class SurfaceEstimate(ctypes.Structure):
@@ -79,6 +79,7 @@ _SIGNATURES = {
     'ss_version': (ctypes.c_char_p, []),
     'ss_last_error': (ctypes.c_char_p, []),
     'ss_workspace_bytes': (ctypes.c_size_t, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32]),
+    'ss_set_rows_per_thread': (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32]),
     'ss_workspace_bytes_slots': (ctypes.c_size_t, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32]),
     'ss_workspace_status': (ctypes.c_int32, [_P, _P]),
     'ss_plan_info': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32,
@@ -113,6 +114,7 @@ _SIGNATURES = {
                                        ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, _P,
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]),
     'ss_batch_min_cluster': (ctypes.c_int32, [ctypes.POINTER(BatchItem), ctypes.c_int32]),
+    'ss_batch_min_cluster_rows': (ctypes.c_int32, [ctypes.POINTER(BatchItem), ctypes.c_int32, ctypes.c_int32]),
     'ss_batch_classes': (ctypes.c_int32, [_P, ctypes.POINTER(BatchClassInfo), ctypes.c_int32,
                                           ctypes.POINTER(ctypes.c_int32)]),
     'ss_batch_run': (ctypes.c_int32, [_P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_int32, _P, _P, _P,

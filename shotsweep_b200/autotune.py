@@ -1,17 +1,22 @@
-"""Autotuner for uneven batches: the cluster size (CTAs per solve) of each size class.
+"""Autotuner for uneven batches: the launch shape of each size class, its cluster
+size (CTAs per solve) and tile height (rows of the band per thread) together.
 
 A size class is the set of models whose smallest fitting cluster is the same
 (``batch.min_cluster``).  A larger cluster cuts each CTA's band of the grid
 (fewer rows per thread block, fewer threads per CTA, more synchronisation per
-cell) and changes how many solves fit on the GPU at once, so the best size
-depends on the grids in the class.  For every class the tuner times the
-class's own models, with their time axes shortened to `sample_nt` steps, at
-the smallest cluster and up to `extra` sizes above it (and 16 for classes of
-10 or more), and keeps the one with
-the most padded cell-steps per second.  Results are cached per device name and
-class signature (in memory, and in a JSON file when `cache_path` is given).
+cell) and changes how many solves fit on the GPU at once; a shorter tile puts
+more threads (warps) on each band, a taller one reuses more vertical
+neighbours from registers and needs fewer threads, so a grid too large for a
+small cluster at one height may fit it at another.  The best pair depends on
+the grids in the class.  For every class the tuner times the class's own
+models, with their time axes shortened to `sample_nt` steps, at tile heights
+4, 5 and 6, each at the smallest cluster that fits every model of the class
+at that height and up to `extra` sizes above it (and 16 when that smallest
+cluster is 10 or more), and keeps the pair with the most padded cell-steps
+per second.  Results are cached per device name and class signature (in
+memory, and in a JSON file when `cache_path` is given).
 
-    table = tune(shapes)                 # {min_cluster: cluster}
+    table = tune(shapes)                 # {min_cluster: (cluster, rows per thread)}
     schedule = tune_schedule(shapes, table)
     batch = UnevenBatch(shapes, clusters=table, schedule=schedule)
 
@@ -29,7 +34,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .batch import Shape, UnevenBatch, min_cluster
+from .batch import TILE_ROWS, UnevenBatch, make_items, min_cluster
 
 _MEMO = {}
 
@@ -48,10 +53,20 @@ def _signature(shapes):
     return (len(shapes), min(nz), max(nz), min(nx), max(nx), sum(s.n_shots for s in shapes))
 
 
-def _time_class(shapes, cluster, c_min, device, sample_nt, reps):
-    """Seconds of one images run of `shapes` (time axes capped at sample_nt) at `cluster`."""
+def smallest_cluster(shape, rows, mode=_lib.MODE_IMAGES):
+    """The smallest cluster that fits one solve of `shape` at `rows` rows per thread (0: none does)."""
+    items, _ = make_items([shape])
+    rc = _lib.load().ss_batch_min_cluster_rows(items, mode, rows)
+    return rc if rc > 0 else 0
+
+
+def _time_class(shapes, shape, c_min, device, sample_nt, reps):
+    """Seconds of one images run of `shapes` (time axes capped at sample_nt) at launch shape
+    (cluster, rows per thread)."""
     short = [dataclasses.replace(s, nt=min(s.nt, sample_nt)) for s in shapes]
-    batch = UnevenBatch(short, device=device, clusters={c_min: cluster}, schedule=0)
+    batch = UnevenBatch(short, device=device, clusters={c_min: shape}, schedule=0)
+    if any((c['cluster'], c['rows_per_thread']) != tuple(shape) for c in batch.classes()):
+        raise RuntimeError('the class does not fit this launch shape')
     rng = np.random.default_rng(0)
     vel = batch.pack_models([np.full((s.nz, s.nx), 2500.0, np.float32) for s in short])
     obs = batch.pack_traces([rng.standard_normal((s.n_shots, s.nt, s.nx)).astype(np.float32) for s in short])
@@ -72,7 +87,7 @@ def _time_class(shapes, cluster, c_min, device, sample_nt, reps):
 
 
 def tune(shapes, device=None, extra=2, sample_nt=192, reps=3, cache_path=None, verbose=False):
-    """{min_cluster: best cluster} for the size classes of `shapes` (images mode)."""
+    """{min_cluster: (best cluster, best rows per thread)} for the size classes of `shapes` (images mode)."""
     device = torch.device('cuda', torch.cuda.current_device()) if device is None else torch.device(device)
     name = torch.cuda.get_device_name(device)
     members = class_members(shapes)
@@ -84,28 +99,34 @@ def tune(shapes, device=None, extra=2, sample_nt=192, reps=3, cache_path=None, v
         sub = [shapes[i] for i in idx]
         key = f'{name}|{c_min}|{_signature(sub)}|{sample_nt}'
         if key in _MEMO or key in cache:
-            table[c_min] = int(_MEMO.get(key, cache.get(key)))
+            table[c_min] = tuple(int(x) for x in _MEMO.get(key, cache.get(key)))
             continue
         best, results = None, {}
-        # sizes just above the smallest, and for large grids the largest cluster,
-        # which may pack the GPU's processing clusters better than one just above
-        sizes = set(range(c_min, min(_lib.MAX_CLUSTER, c_min + extra) + 1))
-        if c_min >= 10:
-            sizes.add(_lib.MAX_CLUSTER)
-        for c in sorted(sizes):
-            try:
-                secs, work = _time_class(sub, c, c_min, device, sample_nt, reps)
-            except RuntimeError:          # this cluster size does not fit: skip it
+        for rows in TILE_ROWS:
+            # the smallest cluster that fits every model of the class at this height, sizes just
+            # above it, and for large grids the largest cluster, which may pack the GPU's processing
+            # clusters better than one just above
+            need = [smallest_cluster(sh, rows) for sh in {(s.nz, s.nx, s.nt, s.pad): s for s in sub}.values()]
+            if min(need) == 0:
                 continue
-            results[c] = work / secs
-            if best is None or results[c] > results[best]:
-                best = c
+            lo = max(need)
+            sizes = set(range(lo, min(_lib.MAX_CLUSTER, lo + extra) + 1))
+            if lo >= 10:
+                sizes.add(_lib.MAX_CLUSTER)
+            for c in sorted(sizes):
+                try:
+                    secs, work = _time_class(sub, (c, rows), c_min, device, sample_nt, reps)
+                except RuntimeError:          # this launch shape does not fit: skip it
+                    continue
+                results[(c, rows)] = work / secs
+                if best is None or results[(c, rows)] > results[best]:
+                    best = (c, rows)
         if best is None:
-            raise RuntimeError(f'no cluster size could run size class {c_min}')
+            raise RuntimeError(f'no launch shape could run size class {c_min}')
         table[c_min] = best
-        _MEMO[key] = best
-        cache[key] = best
-        report[c_min] = {c: f'{r / 1e9:.2f} Gcell-steps/s' for c, r in results.items()}
+        _MEMO[key] = list(best)
+        cache[key] = list(best)
+        report[c_min] = {f'{c}x{h}': f'{r / 1e9:.2f} Gcell-steps/s' for (c, h), r in results.items()}
         if verbose:
             print(f'size class {c_min} ({len(sub)} models): {report[c_min]} -> {best}')
     if cache_path:

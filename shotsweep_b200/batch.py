@@ -78,6 +78,20 @@ def make_items(shapes):
     return items, (vo, to, oo)
 
 
+MAX_CLASSES = 32          # (cluster size, tile height) launches of one plan, at most
+TILE_ROWS = (4, 5, 6)     # tile heights (rows per thread) of the batch kernels
+
+
+def launch_shape_code(shape):
+    """A size class's launch shape for ss_batch_plan: a cluster size, or (cluster size, rows per thread)."""
+    if isinstance(shape, (tuple, list)):
+        c, h = int(shape[0]), int(shape[1])
+        if h not in TILE_ROWS:
+            raise ValueError(f'rows per thread must be one of {TILE_ROWS}')
+        return c | (h << 8)
+    return int(shape)
+
+
 def min_cluster(shape, mode=_lib.MODE_IMAGES):
     """The size class of a model: the smallest cluster of CTAs that fits one of its solves."""
     items, _ = make_items([shape])
@@ -96,6 +110,8 @@ class UnevenBatch:
     SCHEDULES = (0, 1, 2)
 
     def __init__(self, shapes, device=None, clusters=None, schedule=2, phys=None):
+        """clusters: {size class (smallest cluster at 5 rows per thread): cluster size or (cluster size,
+        rows per thread)}, e.g. from autotune.tune; classes not listed run at their smallest cluster."""
         if not shapes:
             raise ValueError('an uneven batch needs at least one model')
         self.shapes = list(shapes)
@@ -122,7 +138,7 @@ class UnevenBatch:
             return self._plans[mode]
         table = (ctypes.c_int32 * (_lib.MAX_CLUSTER + 1))()
         for k, v in self.clusters.items():
-            table[int(k)] = int(v)
+            table[int(k)] = launch_shape_code(v)
         pb, wb = ctypes.c_size_t(0), ctypes.c_size_t(0)
         args = (ctypes.byref(self.phys), mode, self.items, len(self.items), table, self.schedule)
         with torch.cuda.device(self.device):
@@ -136,11 +152,12 @@ class UnevenBatch:
 
     def classes(self, mode=_lib.MODE_IMAGES):
         host, _, _ = self.plan(mode)
-        out = (_lib.BatchClassInfo * _lib.MAX_CLUSTER)()
+        out = (_lib.BatchClassInfo * MAX_CLASSES)()
         n = ctypes.c_int32(0)
-        _lib.check(self.L.ss_batch_classes(host.ctypes.data_as(ctypes.c_void_p), out, _lib.MAX_CLUSTER,
+        _lib.check(self.L.ss_batch_classes(host.ctypes.data_as(ctypes.c_void_p), out, MAX_CLASSES,
                                            ctypes.byref(n)), 'ss_batch_classes')
-        keys = ('min_cluster', 'cluster', 'n_solves', 'threads', 'smem_bytes', 'slots', 'stream', 'cell_steps')
+        keys = ('min_cluster', 'cluster', 'rows_per_thread', 'n_solves', 'threads', 'smem_bytes', 'slots', 'stream',
+                'cell_steps')
         return [{k: getattr(out[i], k) for k in keys} for i in range(n.value)]
 
     def workspace(self, mode):

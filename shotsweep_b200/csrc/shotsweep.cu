@@ -35,6 +35,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -46,8 +47,13 @@
 
 namespace {
 
-constexpr int kRowsPerThread = 5;          // H: rows per thread in the band
-constexpr int kMaxThreads = 384;           // register budget: 168 regs/thread
+// Tile height H (rows of the band per thread) and the CTA size it allows: the
+// register file holds 65,536 registers per SM and a CTA runs alone on its SM,
+// so H x 4 cells at two time levels plus accumulators leave 168 registers per
+// thread at H = 5 (384 threads), 128 at H = 4 (512), 102 at H = 3 (640).
+constexpr int kDefaultRows = 5;
+__host__ __device__ constexpr int max_threads_for(int H) { return H <= 3 ? 640 : H == 4 ? 512 : H == 5 ? 384 : 320; }
+constexpr int kMinRows = 3, kMaxRows = 6;
 constexpr int kMaxCluster = 16;
 constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush (at most)
 constexpr int kMinTraceRing = 8;           // the fewest, for grids whose shared memory is tight
@@ -106,10 +112,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Tensor memory (TMEM) holds the per-cell coefficients of the fixed-geometry
 // kernels: warp w may reach lanes 32*(w%4) .. +31 only, so thread (w, l) owns
-// lane 32*(w%4) + l and columns kCoefColsPerWarp*(w/4) + 8k .. +7 for tile row
-// k: kappa (4 cells), then -sigma (4 cells).
-constexpr uint32_t kCoefColsPerWarp = 40;   // 5 tile rows x 8 words
-constexpr uint32_t kCoefCols = 128;         // 3 warp groups x 40, as a power of two
+// lane 32*(w%4) + l and columns 8H*(w/4) + 8k .. +7 for tile row k: kappa
+// (4 cells), then -sigma (4 cells).
+constexpr uint32_t kCoefCols = 128;         // a power of two >= 8H x warp groups
 __device__ __forceinline__ void tmem_alloc_warp(uint32_t dst_smem, uint32_t ncols) {   // one whole warp
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
                : "memory");
@@ -370,8 +375,8 @@ __device__ __forceinline__ void neg_stencil(const float4& r0, const float4& r1, 
   const float2 zf_hi = __fadd2_rn(make_float2(r0.z, r0.w), make_float2(r4.z, r4.w));
   const float2 xn_lo = make_float2(lf.y + r2.y, r2.x + r2.z);
   const float2 xn_hi = make_float2(r2.y + r2.w, r2.z + rt.x);
-  const float2 xf_lo = make_float2(lf.x + r2.z, lf.y + r2.w);
-  const float2 xf_hi = make_float2(r2.x + rt.x, r2.y + rt.y);
+  const float2 xf_lo = __fadd2_rn(lf, make_float2(r2.z, r2.w));   // aligned pairs: one packed add each
+  const float2 xf_hi = __fadd2_rn(make_float2(r2.x, r2.y), rt);
   const float2 m16 = make_float2(-16.f, -16.f), p60 = make_float2(60.f, 60.f);
   lo = __ffma2_rn(p60, make_float2(r2.x, r2.y), __ffma2_rn(m16, __fadd2_rn(zn_lo, xn_lo), __fadd2_rn(zf_lo, xf_lo)));
   hi = __ffma2_rn(p60, make_float2(r2.z, r2.w), __ffma2_rn(m16, __fadd2_rn(zn_hi, xn_hi), __fadd2_rn(zf_hi, xf_hi)));
@@ -489,9 +494,8 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
 // neighbouring tiles read (the full field of the current level, ping-pong
 // buffered).  The time loop is unrolled by two so that the two register
 // arrays swap roles without moves.
-template <int MODE, bool FAST, bool BATCH>
-__global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) {
-  constexpr int H = kRowsPerThread;
+template <int MODE, bool FAST, bool BATCH, int H>
+__global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KParams P) {
   constexpr bool ADJ = MODE != SS_MODE_FORWARD;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Geometry: compile-time constants on the fast path, parameter-bank reads
@@ -513,9 +517,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
 #define GNACT (BATCH ? gs.nact : P.nact)
 
   // The fixed-geometry instantiations keep the per-cell coefficients in
-  // tensor memory (freeing 40 registers per thread); the uneven batch keeps
-  // them in registers.
-  constexpr bool TC = !BATCH;
+  // tensor memory (freeing 8H registers per thread); the uneven batch keeps
+  // them in registers.  Thread (w, l) owns TMEM lane 32*(w%4) + l and the
+  // 8H columns from 8H*(w/4): kappa (4 cells), then -sigma (4 cells) per
+  // tile row; at most kCoefCols columns for every H <= 5.
+  constexpr bool TC = !BATCH && H <= 5;
+  constexpr uint32_t kColsPerWarp = 8u * H;
+  static_assert(!TC || kColsPerWarp * ((max_threads_for(H) / 32 + 3) / 4) <= kCoefCols, "TMEM columns");
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
   // A 1-D grid of 1-D clusters: the CTA's rank in its cluster and the
@@ -579,7 +587,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) solve_kernel(const KParams P) 
     tmem_fence_after();
     const uint32_t warp = static_cast<uint32_t>(tid >> 5);
     tc_base = *reinterpret_cast<const uint32_t*>(&S.bar[kStages + 2]) + ((32u * (warp & 3u)) << 16) +
-              kCoefColsPerWarp * (warp >> 2);
+              kColsPerWarp * (warp >> 2);
   }
 
   for (int it = slot;; it += n_slots) {
@@ -1308,7 +1316,7 @@ __global__ void __launch_bounds__(256) fp32_probe_kernel(float* out, int iters) 
 // Host side: plans, workspace, launches
 // ----------------------------------------------------------------------------
 struct Plan {
-  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads, ring;
+  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads, ring, H;
   bool fast;
   size_t smem;
   int max_clusters;
@@ -1335,32 +1343,52 @@ using SolveFn = void (*)(KParams);
 // compile-time strides; every other geometry takes them from KParams.
 bool fast_geometry(int nx, int pad) { return nx == 70 && pad == 40; }
 
-SolveFn kernel_for(int mode, bool fast) {
+// Tile heights with fixed-geometry instantiations, and with batch ones.
+bool fixed_rows_ok(int H) { return H == 4 || H == 5; }
+bool batch_rows_ok(int H) { return H >= 4 && H <= 6; }
+
+template <int H>
+SolveFn kernel_for_rows(int mode, bool fast) {
   switch (mode) {
     case SS_MODE_FORWARD:
-      return fast ? solve_kernel<SS_MODE_FORWARD, true, false> : solve_kernel<SS_MODE_FORWARD, false, false>;
+      return fast ? solve_kernel<SS_MODE_FORWARD, true, false, H> : solve_kernel<SS_MODE_FORWARD, false, false, H>;
     case SS_MODE_GRADIENT:
-      return fast ? solve_kernel<SS_MODE_GRADIENT, true, false> : solve_kernel<SS_MODE_GRADIENT, false, false>;
+      return fast ? solve_kernel<SS_MODE_GRADIENT, true, false, H> : solve_kernel<SS_MODE_GRADIENT, false, false, H>;
     case SS_MODE_SEGMENT:
-      return fast ? solve_kernel<SS_MODE_SEGMENT, true, false> : solve_kernel<SS_MODE_SEGMENT, false, false>;
-    default: return fast ? solve_kernel<SS_MODE_IMAGES, true, false> : solve_kernel<SS_MODE_IMAGES, false, false>;
+      return fast ? solve_kernel<SS_MODE_SEGMENT, true, false, H> : solve_kernel<SS_MODE_SEGMENT, false, false, H>;
+    default: return fast ? solve_kernel<SS_MODE_IMAGES, true, false, H> : solve_kernel<SS_MODE_IMAGES, false, false, H>;
   }
 }
+SolveFn kernel_for(int mode, bool fast, int H) {
+  return H == 4 ? kernel_for_rows<4>(mode, fast) : kernel_for_rows<5>(mode, fast);
+}
 
-// Uneven batches: one generic instantiation per mode, geometry per solve.
-SolveFn batch_kernel_for(int mode) {
+// Uneven batches: one generic instantiation per mode and tile height, geometry per solve.
+template <int H>
+SolveFn batch_kernel_rows(int mode) {
   switch (mode) {
-    case SS_MODE_FORWARD: return solve_kernel<SS_MODE_FORWARD, false, true>;
-    case SS_MODE_GRADIENT: return solve_kernel<SS_MODE_GRADIENT, false, true>;
-    default: return solve_kernel<SS_MODE_IMAGES, false, true>;
+    case SS_MODE_FORWARD: return solve_kernel<SS_MODE_FORWARD, false, true, H>;
+    case SS_MODE_GRADIENT: return solve_kernel<SS_MODE_GRADIENT, false, true, H>;
+    default: return solve_kernel<SS_MODE_IMAGES, false, true, H>;
   }
 }
+SolveFn batch_kernel_for(int mode, int H) {
+  return H == 4 ? batch_kernel_rows<4>(mode) : H == 6 ? batch_kernel_rows<6>(mode) : batch_kernel_rows<5>(mode);
+}
 
-size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring) {
+// Tile height of fixed-geometry plans per mode (0: the default), set by a
+// caller's tuner through ss_set_rows_per_thread.
+std::atomic<int> g_rows_pref[4] = {{0}, {0}, {0}, {0}};
+int rows_for_mode(int mode) {
+  const int r = (mode >= 0 && mode < 4) ? g_rows_pref[mode].load() : 0;
+  return fixed_rows_ok(r) ? r : kDefaultRows;
+}
+
+size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring, int H) {
   const size_t field = static_cast<size_t>(bh + 4) * rs;
   const size_t stage = adj ? static_cast<size_t>(bh) * sw : 0;
   return (2 * field + kStages * stage + ((nt + 31) & ~31) + 32 + (kStages + ring) * static_cast<size_t>(nxs) +
-          (kRowsPerThread + 4) * static_cast<size_t>(rs) + kRowsPerThread * static_cast<size_t>(sw)) *
+          (H + 4) * static_cast<size_t>(rs) + H * static_cast<size_t>(sw)) *
              sizeof(float) +
          (kStages + 3) * sizeof(uint64_t);   // barriers, then the TMEM address word
 }
@@ -1368,7 +1396,8 @@ size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring) {
 // The band plan of a geometry: cluster size, band height, threads and shared
 // memory (arithmetic only; make_plan adds what the device can hold at once).
 int plan_shape(const ss_geometry* g, int mode, Plan* p) {
-  constexpr int H = kRowsPerThread;
+  const int H = rows_for_mode(mode);
+  p->H = H;
   const bool adj = mode != SS_MODE_FORWARD;
   p->nzp = g->nz + 2 * g->pad;
   p->nxp = g->nx + 2 * g->pad;
@@ -1376,7 +1405,7 @@ int plan_shape(const ss_geometry* g, int mode, Plan* p) {
   p->rs = 4 * p->ncg + 8;
   p->sw = 4 * p->ncg;
   const int nrows = p->nzp - 4;
-  const int max_nseg = kMaxThreads / p->ncg;
+  const int max_nseg = max_threads_for(H) / p->ncg;
   if (max_nseg < 1) return fail(SS_ERR_UNSUPPORTED, "model too wide for one band of threads");
   bool ok = false;
   for (int C = std::max(1, (nrows + max_nseg * H - 1) / (max_nseg * H)); C <= kMaxCluster; ++C) {
@@ -1386,7 +1415,7 @@ int plan_shape(const ss_geometry* g, int mode, Plan* p) {
     if (C > 1 && bh < 2) continue;
     // the deepest receiver ring that fits (wide grids with long time axes get a shallower one)
     for (int ring = kTraceRing; ring >= kMinTraceRing && !ok; ring /= 2) {
-      const size_t sm = smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj, ring);
+      const size_t sm = smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj, ring, H);
       if (sm <= kMaxSmem) {
         p->C = C;
         p->nseg = nseg;
@@ -1410,7 +1439,7 @@ int plan_shape(const ss_geometry* g, int mode, Plan* p) {
 int make_plan(const ss_geometry* g, int mode, int n_solves, Plan* p) {
   int rc = plan_shape(g, mode, p);
   if (rc) return rc;
-  const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->fast));
+  const void* fn = reinterpret_cast<const void*>(kernel_for(mode, p->fast, p->H));
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(p->smem));
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   if (p->C > 8) {
@@ -1521,7 +1550,7 @@ int launch(const Plan& p, int mode, const KParams& k, cudaStream_t stream) {
   cfg.stream = stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel_for(mode, p.fast), k);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel_for(mode, p.fast, p.H), k);
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaLaunchKernelEx: ") + cudaGetErrorString(e));
   return SS_OK;
 }
@@ -1613,10 +1642,11 @@ int noalloc_scratch(void** out) {
 // A plan is one contiguous blob, identical in host and device memory:
 // BatchPlanHeader, then BatchItemDev[n_items], then int order[n_solves]
 // (per class, solves longest-first).  The header carries the launch shapes.
-constexpr uint64_t kPlanMagic = 0x3230504853535342ull;   // "BSSSHP02"
+constexpr uint64_t kPlanMagic = 0x3330504853535342ull;   // "BSSSHP03"
+constexpr int kMaxClasses = 32;   // (cluster size, tile height) pairs of one plan
 
 struct BatchClassHost {
-  int C, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter, ring;
+  int C, H, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter, ring;
   int max_clusters, idle_sms;   // co-resident clusters alone on the GPU, and the SMs they leave idle
   size_t hist_slot, trace_slot, gpad_slot, grad_slot;   // floats per slot
   size_t ws_off;                                        // bytes: this class's scratch in the workspace
@@ -1628,7 +1658,7 @@ struct BatchPlanHeader {
   int32_t mode, n_items, n_solves, n_classes, max_nt, concurrent;
   int64_t total_bytes, ws_bytes, items_off, order_off;
   double dtdx2, amp_ref, dx, dt;
-  BatchClassHost cls[kMaxCluster];
+  BatchClassHost cls[kMaxClasses];
 };
 
 // Shared memory of a batch launch: the fixed part (barriers, wavelet,
@@ -1638,8 +1668,7 @@ size_t batch_fixed_smem(int nt_max, int nxs, int ring = kMinTraceRing) {
   return (16 + static_cast<size_t>((nt_max + 31) & ~31) + 32 + static_cast<size_t>(kStages + ring) * nxs) *
          sizeof(float);
 }
-size_t batch_solve_smem(int bh, int ncg, bool adj) {
-  constexpr int H = kRowsPerThread;
+size_t batch_solve_smem(int bh, int ncg, bool adj, int H) {
   const size_t rs = 4 * static_cast<size_t>(ncg) + 8, sw = 4 * static_cast<size_t>(ncg);
   return (2 * (bh + 4) * rs + (adj ? kStages * bh * sw : 0) + (H + 4) * rs + H * sw) * sizeof(float);
 }
@@ -1649,9 +1678,9 @@ int item_ncg(const ss_batch_item& it) { return (it.nx + 2 * it.pad - 4 + 3) / 4;
 struct ItemShape {
   int nseg, bh, nact;
 };
-// Band shape of one item at cluster size C; nact > kMaxThreads means it does not fit.
-ItemShape item_shape(const ss_batch_item& it, int C) {
-  constexpr int H = kRowsPerThread;
+// Band shape of one item at cluster size C and tile height H; nact >
+// max_threads_for(H) means it does not fit.
+ItemShape item_shape(const ss_batch_item& it, int C, int H) {
   const int nrows = it.nz + 2 * it.pad - 4;
   const int ncg = item_ncg(it);
   ItemShape s;
@@ -1660,11 +1689,11 @@ ItemShape item_shape(const ss_batch_item& it, int C) {
   s.nact = ncg * s.nseg;
   return s;
 }
-bool item_fits(const ss_batch_item& it, int C, bool adj) {
-  const ItemShape s = item_shape(it, C);
+bool item_fits(const ss_batch_item& it, int C, bool adj, int H = kDefaultRows) {
+  const ItemShape s = item_shape(it, C, H);
   const int ncg = item_ncg(it);
-  return s.nact <= kMaxThreads &&
-         batch_fixed_smem(it.nt, (it.nx + 3) & ~3) + batch_solve_smem(s.bh, ncg, adj) <= kMaxSmem;
+  return s.nact <= max_threads_for(H) &&
+         batch_fixed_smem(it.nt, (it.nx + 3) & ~3) + batch_solve_smem(s.bh, ncg, adj, H) <= kMaxSmem;
 }
 
 struct DeviceStreams {
@@ -1695,15 +1724,16 @@ int device_streams(DeviceStreams** out) {
 // device, raised (never lowered) as plans need more; a run whose plan set it
 // already makes no attribute call.
 std::mutex g_attr_mutex;
-int g_batch_smem[64][3] = {};
-int ensure_batch_smem(int mode, int bytes) {
+int g_batch_smem[64][3][kMaxRows + 1] = {};
+int ensure_batch_smem(int mode, int H, int bytes) {
   int dev = 0;
   SS_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(SS_ERR_UNSUPPORTED, "device index beyond 63");
+  if (!batch_rows_ok(H)) return fail(SS_ERR_INVALID, "rows per thread of a batch class must lie in 4..6");
   std::lock_guard<std::mutex> lock(g_attr_mutex);
-  int& cur = g_batch_smem[dev][mode];
+  int& cur = g_batch_smem[dev][mode][H];
   if (bytes <= cur) return SS_OK;
-  const void* fn = reinterpret_cast<const void*>(batch_kernel_for(mode));
+  const void* fn = reinterpret_cast<const void*>(batch_kernel_for(mode, H));
   SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
   SS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   cur = bytes;
@@ -1731,8 +1761,10 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
       !(phys->vmax_damping > 0.0) || !(phys->amp_ref > 0.0))
     return fail(SS_ERR_INVALID, "dx, dt, vmax_damping and amp_ref must be positive and 0 < r_coef < 1");
   const bool adj = mode != SS_MODE_FORWARD;
-  // ---- size class of every item: its smallest fitting cluster ------------
-  std::vector<int> cl(n_items), min_c(n_items);
+  // ---- size class of every item: its smallest fitting cluster at the
+  // default tile height; the caller's table maps a size class to a cluster
+  // size (bits 0-7) and a tile height (bits 8-15, 0: the default) -----------
+  std::vector<int> cl(n_items), rows(n_items), min_c(n_items);
   long long n_solves = 0;
   int max_nt = 0;
   for (int i = 0; i < n_items; ++i) {
@@ -1742,9 +1774,20 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
     while (C <= kMaxCluster && !item_fits(items[i], C, adj)) ++C;
     if (C > kMaxCluster) return fail(SS_ERR_UNSUPPORTED, "item " + std::to_string(i) + ": no cluster plan fits this grid");
     min_c[i] = C;
-    int use = C;
-    if (cluster_by_class && cluster_by_class[C] > 0) use = std::min(kMaxCluster, std::max(C, cluster_by_class[C]));
+    int use = C, H = kDefaultRows;
+    if (cluster_by_class && cluster_by_class[C] > 0) {
+      use = std::min(kMaxCluster, std::max(C, cluster_by_class[C] & 0xff));
+      const int hr = (cluster_by_class[C] >> 8) & 0xff;
+      if (hr) {
+        if (!batch_rows_ok(hr)) return fail(SS_ERR_INVALID, "rows per thread of a batch class must lie in 4..6");
+        H = hr;
+      }
+    }
+    while (use <= kMaxCluster && !item_fits(items[i], use, adj, H)) ++use;   // a tile height may need more CTAs
+    if (use > kMaxCluster)
+      return fail(SS_ERR_UNSUPPORTED, "item " + std::to_string(i) + ": no cluster plan fits at this tile height");
     cl[i] = use;
+    rows[i] = H;
     n_solves += items[i].n_shots;
     max_nt = std::max(max_nt, items[i].nt);
   }
@@ -1752,47 +1795,51 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
   // ---- classes by cluster size; a class whose combined shared memory does
   // not fit moves its largest items one cluster size up ---------------------
   BatchPlanHeader h{};
-  std::vector<std::vector<int>> members(kMaxCluster + 1);
-  for (int i = 0; i < n_items; ++i) members[cl[i]].push_back(i);
-  for (int C = 1; C <= kMaxCluster; ++C) {
-    for (;;) {
-      auto& m = members[C];
-      if (m.empty()) break;
-      int nt_max = 0, nxs = 0;
-      size_t solve_part = 0;
-      for (int i : m) {
-        nt_max = std::max(nt_max, items[i].nt);
-        nxs = std::max(nxs, (items[i].nx + 3) & ~3);
-        const ItemShape s = item_shape(items[i], C);
-        solve_part = std::max(solve_part, batch_solve_smem(s.bh, item_ncg(items[i]), adj));
+  // members[H][C]: the items launched at cluster size C and tile height H
+  std::vector<std::vector<std::vector<int>>> members(kMaxRows + 1, std::vector<std::vector<int>>(kMaxCluster + 1));
+  for (int i = 0; i < n_items; ++i) members[rows[i]][cl[i]].push_back(i);
+  for (int H = kMinRows; H <= kMaxRows; ++H)
+    for (int C = 1; C <= kMaxCluster; ++C) {
+      for (;;) {
+        auto& m = members[H][C];
+        if (m.empty()) break;
+        int nt_max = 0, nxs = 0;
+        size_t solve_part = 0;
+        for (int i : m) {
+          nt_max = std::max(nt_max, items[i].nt);
+          nxs = std::max(nxs, (items[i].nx + 3) & ~3);
+          const ItemShape s = item_shape(items[i], C, H);
+          solve_part = std::max(solve_part, batch_solve_smem(s.bh, item_ncg(items[i]), adj, H));
+        }
+        if (batch_fixed_smem(nt_max, nxs) + solve_part <= kMaxSmem) break;
+        if (C == kMaxCluster) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits the batch's shared memory");
+        std::vector<int> keep;
+        for (int i : m) {
+          const ItemShape s = item_shape(items[i], C, H);
+          if (batch_solve_smem(s.bh, item_ncg(items[i]), adj, H) == solve_part)
+            members[H][C + 1].push_back(i);
+          else
+            keep.push_back(i);
+        }
+        if (keep.size() == m.size()) return fail(SS_ERR_UNSUPPORTED, "batch planner made no progress");
+        m.swap(keep);
       }
-      if (batch_fixed_smem(nt_max, nxs) + solve_part <= kMaxSmem) break;
-      if (C == kMaxCluster) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits the batch's shared memory");
-      std::vector<int> keep;
-      for (int i : m) {
-        const ItemShape s = item_shape(items[i], C);
-        if (batch_solve_smem(s.bh, item_ncg(items[i]), adj) == solve_part)
-          members[C + 1].push_back(i);
-        else
-          keep.push_back(i);
-      }
-      if (keep.size() == m.size()) return fail(SS_ERR_UNSUPPORTED, "batch planner made no progress");
-      m.swap(keep);
     }
-  }
   // ---- launch shape, solve order and scratch of every class -------------
   struct Cls {
-    int C;
+    int C, H;
     std::vector<int> items;
     double work;
   };
   std::vector<Cls> cls;
-  for (int C = 1; C <= kMaxCluster; ++C)
-    if (!members[C].empty()) {
-      double work = 0;
-      for (int i : members[C]) work += static_cast<double>(items[i].nt) * items[i].n_shots * C;
-      cls.push_back({C, members[C], work});
-    }
+  for (int H = kMinRows; H <= kMaxRows; ++H)
+    for (int C = 1; C <= kMaxCluster; ++C)
+      if (!members[H][C].empty()) {
+        double work = 0;
+        for (int i : members[H][C]) work += static_cast<double>(items[i].nt) * items[i].n_shots * C;
+        cls.push_back({C, H, members[H][C], work});
+      }
+  if (cls.size() > static_cast<size_t>(kMaxClasses)) return fail(SS_ERR_UNSUPPORTED, "more than 32 batch classes");
   // Heaviest class first: it starts on the whole GPU; lighter ones fill tails.
   std::stable_sort(cls.begin(), cls.end(), [](const Cls& a, const Cls& b) { return a.work > b.work; });
   h.magic = kPlanMagic;
@@ -1811,15 +1858,15 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
   h.order_off = static_cast<int64_t>(align_up(h.items_off + sizeof(BatchItemDev) * static_cast<size_t>(n_items)));
   h.total_bytes = static_cast<int64_t>(align_up(h.order_off + sizeof(int) * static_cast<size_t>(n_solves)));
 
-  const SolveFn fn_ptr = batch_kernel_for(mode);
-  const void* fn = reinterpret_cast<const void*>(fn_ptr);
   std::vector<int> order;
   order.reserve(n_solves);
   size_t region[2] = {0, 0};
   for (size_t c = 0; c < cls.size(); ++c) {
     BatchClassHost& k = h.cls[c];
-    const int C = cls[c].C;
+    const int C = cls[c].C, H = cls[c].H;
+    const void* fn = reinterpret_cast<const void*>(batch_kernel_for(mode, H));
     k.C = C;
+    k.H = H;
     k.min_C = kMaxCluster;
     k.counter = static_cast<int>(c);
     int max_nact = 0;
@@ -1830,11 +1877,11 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
     k.cell_steps = 0;
     for (int i : cls[c].items) {
       const ss_batch_item& it = items[i];
-      const ItemShape s = item_shape(it, C);
+      const ItemShape s = item_shape(it, C, H);
       const int ncg = item_ncg(it);
       k.min_C = std::min(k.min_C, min_c[i]);
       max_nact = std::max(max_nact, s.nact);
-      solve_part = std::max(solve_part, batch_solve_smem(s.bh, ncg, adj));
+      solve_part = std::max(solve_part, batch_solve_smem(s.bh, ncg, adj, H));
       k.nt_max = std::max(k.nt_max, it.nt);
       k.nxs = std::max(k.nxs, (it.nx + 3) & ~3);
       k.bh_max = std::max(k.bh_max, s.bh);
@@ -1862,7 +1909,7 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
     k.order_begin = begin;
     k.n_solves = static_cast<int>(order.size()) - begin;
     // persistent clusters: as many as fit on the device at once
-    int rc = ensure_batch_smem(mode, k.smem);
+    int rc = ensure_batch_smem(mode, H, k.smem);
     if (rc) return rc;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -1958,9 +2005,9 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
     d.vmute = it.v_mute;
     dv[i] = d;
   }
-  for (size_t c = 0; c < cls.size(); ++c)   // band shape at the class's cluster size
+  for (size_t c = 0; c < cls.size(); ++c)   // band shape at the class's cluster size and tile height
     for (int i : cls[c].items) {
-      const ItemShape s = item_shape(items[i], cls[c].C);
+      const ItemShape s = item_shape(items[i], cls[c].C, cls[c].H);
       dv[i].nseg = s.nseg;
       dv[i].bh = s.bh;
       dv[i].nact = s.nact;
@@ -1992,15 +2039,12 @@ int batch_run(const void* plan, const void* plan_dev, const float* vel, const fl
   const unsigned char* pd = static_cast<const unsigned char*>(plan_dev);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   SS_CUDA(cudaMemsetAsync(w, 0, 256, st));
-  const SolveFn fn_ptr = batch_kernel_for(mode);
-  int max_smem = 0;
   bool two = false;
   for (int c = 0; c < h.n_classes; ++c) {
-    max_smem = std::max(max_smem, h.cls[c].smem);
+    rc = ensure_batch_smem(mode, h.cls[c].H, h.cls[c].smem);
+    if (rc) return rc;
     two = two || h.cls[c].stream == 1;
   }
-  rc = ensure_batch_smem(mode, max_smem);
-  if (rc) return rc;
   if (two) {
     SS_CUDA(cudaEventRecord(ds->fork, st));
     SS_CUDA(cudaStreamWaitEvent(ds->side, ds->fork, 0));
@@ -2059,7 +2103,7 @@ int batch_run(const void* plan, const void* plan_dev, const float* vel, const fl
     cfg.stream = k.stream ? ds->side : st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn_ptr, p);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, batch_kernel_for(mode, k.H), p);
     if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaLaunchKernelEx: ") + cudaGetErrorString(e));
   }
   if (two) {
@@ -2090,6 +2134,14 @@ size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mod
   Plan p;
   if (make_plan(geom, mode, n_models * geom->n_shots, &p)) return 0;
   return ws_layout(geom, p, mode).total;
+}
+
+int32_t ss_set_rows_per_thread(int32_t mode, int32_t rows) {
+  g_last_error.clear();
+  if (mode < 0 || mode > 3) return fail(SS_ERR_INVALID, "mode must lie in 0..3");
+  if (rows != 0 && !fixed_rows_ok(rows)) return fail(SS_ERR_INVALID, "rows per thread must be 4 or 5 (0: default)");
+  g_rows_pref[mode].store(rows);
+  return SS_OK;
 }
 
 size_t ss_workspace_bytes_slots(const ss_geometry* geom, int32_t mode, int32_t slots) {
@@ -2125,7 +2177,7 @@ int32_t ss_plan_info(const ss_geometry* geom, int32_t n_models, int32_t mode, in
   out[2] = static_cast<int64_t>(p.smem);
   out[3] = p.bh;
   out[4] = p.ncg;
-  out[5] = kRowsPerThread;
+  out[5] = p.H;
   out[6] = p.max_clusters;
   out[7] = p.slots;
   return SS_OK;
@@ -2425,6 +2477,17 @@ int32_t ss_batch_min_cluster(const ss_batch_item* item, int32_t mode) {
   return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits this grid");
 }
 
+int32_t ss_batch_min_cluster_rows(const ss_batch_item* item, int32_t mode, int32_t rows) {
+  g_last_error.clear();
+  if (!item) return fail(SS_ERR_INVALID, "item is NULL");
+  if (!batch_rows_ok(rows)) return fail(SS_ERR_INVALID, "rows per thread of a batch class must lie in 4..6");
+  int rc = check_item(*item, 0);
+  if (rc) return rc;
+  for (int C = 1; C <= kMaxCluster; ++C)
+    if (item_fits(*item, C, mode != SS_MODE_FORWARD, rows)) return C;
+  return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits this grid at this tile height");
+}
+
 int32_t ss_batch_classes(const void* plan, ss_batch_class_info* out, int32_t max_classes, int32_t* n_classes) {
   g_last_error.clear();
   if (!plan || !n_classes || (max_classes > 0 && !out)) return fail(SS_ERR_INVALID, "bad arguments");
@@ -2442,7 +2505,7 @@ int32_t ss_batch_classes(const void* plan, ss_batch_class_info* out, int32_t max
     o.smem_bytes = k.smem;
     o.slots = k.slots;
     o.stream = k.stream;
-    o.reserved = 0;
+    o.rows_per_thread = k.H;
     o.cell_steps = k.cell_steps;
   }
   return SS_OK;
