@@ -375,8 +375,8 @@ __device__ __forceinline__ void neg_stencil(const float4& r0, const float4& r1, 
   const float2 zf_hi = __fadd2_rn(make_float2(r0.z, r0.w), make_float2(r4.z, r4.w));
   const float2 xn_lo = make_float2(lf.y + r2.y, r2.x + r2.z);
   const float2 xn_hi = make_float2(r2.y + r2.w, r2.z + rt.x);
-  const float2 xf_lo = __fadd2_rn(lf, make_float2(r2.z, r2.w));   // aligned pairs: one packed add each
-  const float2 xf_hi = __fadd2_rn(make_float2(r2.x, r2.y), rt);
+  const float2 xf_lo = make_float2(lf.x + r2.z, lf.y + r2.w);
+  const float2 xf_hi = make_float2(r2.x + rt.x, r2.y + rt.y);
   const float2 m16 = make_float2(-16.f, -16.f), p60 = make_float2(60.f, 60.f);
   lo = __ffma2_rn(p60, make_float2(r2.x, r2.y), __ffma2_rn(m16, __fadd2_rn(zn_lo, xn_lo), __fadd2_rn(zf_lo, xf_lo)));
   hi = __ffma2_rn(p60, make_float2(r2.z, r2.w), __ffma2_rn(m16, __fadd2_rn(zn_hi, xn_hi), __fadd2_rn(zf_hi, xf_hi)));

@@ -137,13 +137,34 @@ def test_graph_replay_equals_eager(case):
     assert torch.equal(img, case['img']) and torch.equal(illum, case['illum'])
 
 
-def test_autotuner_picks_a_fitting_cluster_per_class():
+def test_autotuner_picks_a_fitting_launch_shape_per_class():
+    """The tuner's table gives every size class a (cluster size, tile height) pair from the candidates it
+    times: a tile height of 4-6 rows and a cluster from the smallest that fits every model of the class at
+    that height to one above it (or 16 for classes of large grids)."""
     from shotsweep_b200 import autotune
+    from shotsweep_b200.batch import TILE_ROWS
     shs = shapes()[:5]
     table = autotune.tune(shs, sample_nt=64, reps=1, extra=1)
     members = autotune.class_members(shs)
     assert set(table) == set(members)
-    assert all(c_min <= c <= c_min + 1 or (c_min >= 10 and c == 16) for c_min, c in table.items())
+    for c_min, (c, rows) in table.items():
+        assert rows in TILE_ROWS
+        lo = max(autotune.smallest_cluster(shs[i], rows) for i in members[c_min])
+        assert lo <= c <= lo + 1 or (lo >= 10 and c == 16), (c_min, c, rows, lo)
+
+
+def test_tile_heights_do_not_change_results(case):
+    """Every class forced to 4 and to 6 rows per thread (at the smallest cluster that fits) gives the
+    same images and illumination, bit for bit: a cell's arithmetic does not depend on the tile."""
+    from shotsweep_b200.batch import UnevenBatch
+    b = case['batch']
+    for rows in (4, 6):
+        table = {c['min_cluster']: (c['min_cluster'], rows) for c in b.classes()}
+        alt = UnevenBatch(case['shapes'], clusters=table, schedule=0)
+        assert all(c['rows_per_thread'] == rows for c in alt.classes())
+        img, illum, _ = alt.images(case['vb'], case['wav'], case['obs'], t_mute=0.03)
+        alt.status()
+        assert torch.equal(img, case['img']) and torch.equal(illum, case['illum']), rows
 
 
 def test_batch_rejects_bad_input(case):

@@ -137,6 +137,38 @@ def test_process_batch_stays_within_memory_budget(gpu):
     assert np.array_equal(img, ref_img.cpu().numpy()) and np.array_equal(illum, ref_illum.cpu().numpy())
 
 
+def test_tile_height_does_not_change_results(gpu):
+    """Plans at 4 rows per thread (512 threads per CTA) give the same gathers, images and illumination as
+    the default 5 (384 threads), bit for bit, on the OpenFWI grid and on an odd one."""
+    import ctypes
+    from shotsweep_b200 import _lib, engine, synth
+    L = _lib.load()
+    for geom_args in ((70, 70, 300, 40, (0, 17, 34, 52, 69)), (23, 37, 160, 9, (0, 18, 36))):
+        nz, nx = geom_args[:2]
+        eng = engine.Engine(engine.geometry(*geom_args))
+        dev = eng.device
+        f32 = dict(dtype=torch.float32, device=dev)
+        truth = torch.tensor(np.stack([synth.model('curved', [7, i], nz, nx) for i in range(2)]), **f32)
+        bg = torch.tensor(np.stack([np.tile(np.linspace(1700, 3300, nz)[:, None], (1, nx))] * 2), **f32)
+        w = engine.scaled_wavelet(np.sin(np.arange(geom_args[2]) * 0.2) * np.exp(-np.arange(geom_args[2]) / 30.0), dev)
+        out = {}
+        try:
+            for rows in (5, 4):
+                for mode in range(4):
+                    assert L.ss_set_rows_per_thread(mode, rows) == 0
+                assert eng.plan(2, _lib.MODE_IMAGES)['rows_per_thread'] == rows
+                obs = eng.forward(truth, w)
+                img, illum = eng.images(bg, w, obs, torch.tensor([1800.0, 1900.0], **f32))
+                eng.status()
+                out[rows] = (obs, img, illum)
+        finally:
+            for mode in range(4):
+                L.ss_set_rows_per_thread(mode, 0)
+        for a, b in zip(out[5], out[4]):
+            assert torch.equal(a, b), geom_args
+    assert L.ss_set_rows_per_thread(2, 3) == _lib.ERR_INVALID
+
+
 def test_forward_returns_reference_structures(gpu, plain):
     sim = gpu.Sim(checkpoint_interval=250)
     out, ck, c2 = sim.forward(plain['model'][None], store=True)
