@@ -336,9 +336,11 @@ def run_ours(args):
         sim.images(bgs, obs_host, v_mute=vm)
     e2e_s = D.reduce(time.perf_counter() - t0, 'max', dev if world > 1 else None)
     e2e = world * shot_images * e2e_steps / e2e_s
-    # the same call with pageable NumPy gathers (what the reference's callers pass)
+    # the same call with pageable NumPy gathers (what the reference's callers pass); the first call
+    # allocates the pinned staging buffers (the host allocator keeps them for later calls)
     obs_np = obs_host.numpy().copy()
     del obs_host
+    sim.images(bgs, obs_np, v_mute=vm)
     D.barrier()
     t0 = time.perf_counter()
     for _ in range(2):
@@ -349,6 +351,8 @@ def run_ours(args):
     per_call = int(2.0 * 1024 ** 3 // gpu.imaging_memory_bytes(len(RHOS)))
     obs_models = obs_np[::len(RHOS)].astype(np.float64)
     del obs_np
+    sim.images(bgs[:per_call * len(RHOS)], np.repeat(obs_models[:per_call], len(RHOS), 0),
+               v_mute=vm[:per_call * len(RHOS)])
     D.barrier()
     t0 = time.perf_counter()
     for i in range(0, per, per_call):
@@ -502,7 +506,8 @@ def run_uneven(args):
                        'padded_cell_steps_per_gpu': cell_steps,
                        'l2': f'inputs larger than L2 ({obs.numel() * 4 / 1e9:.1f} GB of gathers per step per GPU)',
                        'autotune': {str(k): v for k, v in sorted(table.items())}, 'schedule': schedule,
-                       'classes': [{k: c[k] for k in ('min_cluster', 'cluster', 'n_solves', 'threads', 'slots',
+                       'classes': [{k: c[k] for k in ('min_cluster', 'cluster', 'rows_per_thread', 'n_solves', 'threads',
+                                                      'slots',
                                                       'stream')} for c in classes]},
             'roofline': {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s',
                          'frac': achieved / peak, 'traffic': None,
@@ -625,6 +630,7 @@ def run_learned(args):
                                    f'{args.test_models} held-out models, L-BFGS iterations per band '
                                    f'{iters} (bands {bands}: Hz of the low-pass, None = full band)',
                        'parameters': 2961536},
+            'time_ratio_inclusive': res['time_ratio_inclusive'],
             'plain_fwi_seconds': res['plain_seconds'], 'learned_time_to_plain_misfit_s': res['learned_time_to_plain_misfit'],
             'propose_seconds': res['propose_seconds'], 'train_seconds': res['train_seconds'],
             'train_steps_per_s': res['train_steps_per_s'], 'data_seconds': res['data_seconds'],

@@ -18,9 +18,15 @@
 5. ``fwi.BatchFWI.run_bands`` from both starts: L-BFGS for `iters` iterations in the full band
    (an int), or the reference's multiscale schedule (fwi.py:138-163: `bands` such as an 8 Hz
    low-pass then the full band, `iters` per band, each model with its own Wiener-estimated wavelet
-   per band).  The time-to-misfit is the wall time the learned start (inference and acceptance
-   included) needs to reach plain FWI's final full-band total misfit, against plain FWI's own wall
-   time; only full-band misfits are compared.
+   per band).  Plain FWI runs the schedule as given.  With several bands the learned method runs
+   it only for the models whose proposal was refused (the fallback is plain FWI, from the
+   background, every band); an accepted proposal already holds the long wavelengths that the
+   low band exists to recover, so its model goes straight to the full band, with as many
+   iterations as the whole schedule.  The fallback group runs first, so its time counts in full.
+   The time-to-misfit is the wall time the learned start (inference and acceptance included)
+   needs to reach plain FWI's final full-band total misfit over all held-out models, against
+   plain FWI's own wall time; only full-band misfits are compared.  `time_ratio_inclusive` adds
+   the data simulation and the training to the learned side.
 """
 from __future__ import annotations
 
@@ -100,6 +106,32 @@ def norm_mae(v, truth):
     return float(np.abs(a - b).mean())
 
 
+def learned_multiscale(eng, w, obs, prop, bg, use, bands, iters, propose_s):
+    """The learned side of a multiscale run: refused proposals fall back to plain FWI over every band
+    (run first), accepted ones go straight to the full band for sum(iters) iterations.  Returns the
+    final models and the curve [(seconds since the proposal started, total full-band misfit)]."""
+    acc, rej = np.flatnonzero(use), np.flatnonzero(~use)
+    dev = obs.device
+    v = torch.empty_like(bg)
+    t_rej, j_rej = 0.0, 0.0
+    if len(rej):
+        ri = torch.tensor(rej, device=dev)
+        v_r, h_r = BatchFWI(eng, w, obs[ri].contiguous()).run_bands(bg[ri].contiguous(), gpu.RICKER, bands, iters)
+        v[ri] = v_r
+        t_rej = h_r[-1][0]
+        j_rej = float(h_r[-1][1].sum())
+    curve = [(propose_s + t_rej, float('inf'))]
+    if len(acc):
+        ai = torch.tensor(acc, device=dev)
+        v_a, h_a = BatchFWI(eng, w, obs[ai].contiguous()).run_bands(prop[ai].contiguous(), gpu.RICKER,
+                                                                   (bands[-1],), (int(sum(iters)),))
+        v[ai] = v_a
+        curve = [(propose_s + t_rej + h[0], j_rej + float(h[1].sum())) for h in h_a]
+    else:
+        curve = [(propose_s + t_rej, j_rej)]
+    return v, curve
+
+
 def run(n_train=20000, n_test=256, steps=6000, batch=64, iters=50, bands=None, seed=0, train_tag=101,
         test_tag=202, log=print):
     dev = torch.device('cuda', torch.cuda.current_device())
@@ -150,16 +182,22 @@ def run(n_train=20000, n_test=256, steps=6000, batch=64, iters=50, bands=None, s
     if bands is None or len(bands) != len(iters):
         raise ValueError('give one iteration count per band')
     v_plain, h_plain = BatchFWI(eng, w, obs).run_bands(bg, gpu.RICKER, bands, iters)
-    v_learn, h_learn = BatchFWI(eng, w, obs).run_bands(start, gpu.RICKER, bands, iters)
     last = len(bands) - 1
     plain_total = [float(h[1].sum()) for h in h_plain if h[2] == last]
-    learn_total = [float(h[1].sum()) for h in h_learn if h[2] == last]
     target = plain_total[-1]
     t_plain = h_plain[-1][0]
-    reach = next((propose_s + h[0] for h in h_learn if h[2] == last and float(h[1].sum()) <= target), None)
+    if len(bands) == 1:
+        v_learn, h_learn = BatchFWI(eng, w, obs).run_bands(start, gpu.RICKER, bands, iters)
+        curve = [(propose_s + h[0], float(h[1].sum())) for h in h_learn]
+    else:
+        v_learn, curve = learned_multiscale(eng, w, obs, prop, bg, use, bands, iters, propose_s)
+    learn_total = [j for _, j in curve]
+    reach = next((t for t, j in curve if j <= target), None)
     res.update(plain_final_misfit=target, learned_final_misfit=learn_total[-1], plain_seconds=t_plain,
-               learned_seconds=h_learn[-1][0] + propose_s, learned_time_to_plain_misfit=reach,
+               learned_seconds=curve[-1][0], learned_time_to_plain_misfit=reach,
                time_ratio=None if reach is None else reach / t_plain,
+               time_ratio_inclusive=None if reach is None else
+               (res['data_seconds'] + res['train_seconds'] + reach) / t_plain,
                plain_misfit_curve=plain_total, learned_misfit_curve=learn_total,
                mae_plain_fwi=norm_mae(v_plain.cpu().numpy(), test_models),
                mae_learned_fwi=norm_mae(v_learn.cpu().numpy(), test_models))
