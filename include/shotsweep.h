@@ -410,6 +410,10 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
  *                         sum of the column gradients dcols [pixels_out][Kc]
  *                         that read input element (pixel, c); y: the input map
  *   ss_transpose_bf16     out[c][r] = in[r][c]
+ *   ss_transpose_sum_bf16 the same, and colsum[c] += sum over rows of in[r][c]
+ *                         in the same pass (a layer's bias gradient from its
+ *                         pre-activation gradient while that is transposed for
+ *                         the weight-gradient GEMM)
  *   ss_bias_grad_bf16     db[c] += sum over rows of dpre[row][c]
  * Output head: crop [off, off+n)^2 of x [B][H][W][C], 3x3 convolution with
  * zero padding, bias, tanh; head[6] = {B, H, W, C, off, n}; weights w[9][C].
@@ -426,6 +430,8 @@ int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t t
 int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
                              void* dpre, int64_t ldp, void* stream);
 int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream);
+int32_t ss_transpose_sum_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out,
+                              float* colsum, void* stream);
 int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream);
 int32_t ss_head_forward(const void* x, const int32_t* head, const float* w, const float* bias, float* out, void* stream);
 int32_t ss_head_backward(const void* x, const int32_t* head, const float* w, const float* dpre, float slope, float* dw,

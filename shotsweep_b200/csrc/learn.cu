@@ -410,6 +410,73 @@ __global__ void transpose_bf16_kernel(const bf16* __restrict__ in, int64_t ld_in
   }
 }
 
+// out[c][r] = in[r][c] for a [R][C] BF16 matrix (row strides ld_in, ld_out, both
+// even), in 64 x 64 tiles: rows are read and written as BF16 pairs (4-byte
+// accesses), staged in shared memory.  With colsum != NULL the block also adds
+// the column sums of its rows into colsum (float), one atomic per column per
+// block: a CTA walks `tiles` row tiles so that the atomics stay few.
+constexpr int kTT = 64;
+__global__ void __launch_bounds__(256) transpose_sum_kernel(const bf16* __restrict__ in, int64_t ld_in, int R, int C,
+                                                            bf16* __restrict__ out, int64_t ld_out,
+                                                            float* __restrict__ colsum, int tiles) {
+  __shared__ bf16 tile[kTT][kTT + 2];
+  __shared__ float part[8][kTT];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int c0 = blockIdx.x * kTT;
+  const int c = c0 + 2 * tx;
+  float s0 = 0.f, s1 = 0.f;
+  for (int t = 0; t < tiles; ++t) {
+    const int64_t r0 = (static_cast<int64_t>(blockIdx.y) * tiles + t) * kTT;
+    if (r0 >= R) break;
+    for (int j = ty; j < kTT; j += 8) {
+      const int64_t r = r0 + j;
+      bf16 a = __float2bfloat16(0.f), b = a;
+      if (r < R) {
+        const bf16* p = in + r * ld_in + c;
+        if (c + 1 < C) {
+          const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(p);
+          a = v.x;
+          b = v.y;
+        } else if (c < C) {
+          a = p[0];
+        }
+      }
+      tile[j][2 * tx] = a;
+      tile[j][2 * tx + 1] = b;
+      s0 += __bfloat162float(a);
+      s1 += __bfloat162float(b);
+    }
+    __syncthreads();
+    for (int j = ty; j < kTT; j += 8) {
+      const int cc = c0 + j;
+      const int64_t r = r0 + 2 * tx;
+      if (cc < C && r < R) {
+        bf16* q = out + static_cast<int64_t>(cc) * ld_out + r;
+        if (r + 1 < R) {
+          __nv_bfloat162 v;
+          v.x = tile[2 * tx][j];
+          v.y = tile[2 * tx + 1][j];
+          *reinterpret_cast<__nv_bfloat162*>(q) = v;
+        } else {
+          q[0] = tile[2 * tx][j];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (colsum) {
+    part[ty][2 * tx] = s0;
+    part[ty][2 * tx + 1] = s1;
+    __syncthreads();
+    if (threadIdx.x < kTT && c0 + threadIdx.x < C) {
+      float s = 0.f;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s += part[k][threadIdx.x];
+      atomicAdd(colsum + c0 + threadIdx.x, s);
+    }
+  }
+}
+
 // db[c] += sum over rows of dpre[row][c]
 __global__ void bias_grad_kernel(const bf16* __restrict__ dpre, int64_t ld, int64_t M, int C, float* __restrict__ db) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -664,14 +731,46 @@ int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc
   return SS_OK;
 }
 
+// Transpose (and optionally column sums) through the pair-wise kernel when
+// strides and addresses allow 4-byte BF16-pair accesses, else element-wise.
+static int transpose_launch(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, float* colsum,
+                     void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool pairs = (ld_in % 2 == 0) && (ld_out % 2 == 0) && (reinterpret_cast<uintptr_t>(in) % 4 == 0) &&
+                     (reinterpret_cast<uintptr_t>(out) % 4 == 0);
+  if (pairs) {
+    const int gx = (C + kTT - 1) / kTT;
+    const long long row_tiles = (static_cast<long long>(R) + kTT - 1) / kTT;
+    // with column sums, enough row tiles per CTA that about 4 CTAs per SM remain (few atomics per column)
+    const int tiles = colsum ? static_cast<int>(std::max<long long>(1, row_tiles * gx / 592)) : 1;
+    const long long gy = (row_tiles + tiles - 1) / tiles;
+    if (gy > 65535) return fail(SS_ERR_UNSUPPORTED, "matrix too tall to transpose");
+    transpose_sum_kernel<<<dim3(gx, static_cast<unsigned>(gy)), 256, 0, st>>>(
+        static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out), ld_out, colsum, tiles);
+  } else {
+    dim3 grid((C + 31) / 32, (R + 31) / 32);
+    transpose_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C,
+                                                          static_cast<bf16*>(out), ld_out);
+    if (colsum) {
+      dim3 g2((C + 127) / 128, static_cast<unsigned>(std::min<long long>(R, 512)));
+      bias_grad_kernel<<<g2, 128, 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C, colsum);
+    }
+  }
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
 int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream) {
   ss_internal::clear_error();
   if (!in || !out || R < 1 || C < 1 || ld_in < C || ld_out < R) return fail(SS_ERR_INVALID, "bad arguments");
-  dim3 grid((C + 31) / 32, (R + 31) / 32);
-  transpose_bf16_kernel<<<grid, dim3(32, 8), 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out), ld_out);
-  SS_TRY_CUDA(cudaGetLastError());
-  return SS_OK;
+  return transpose_launch(in, ld_in, R, C, out, ld_out, nullptr, stream);
+}
+
+int32_t ss_transpose_sum_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out,
+                              float* colsum, void* stream) {
+  ss_internal::clear_error();
+  if (!in || !out || !colsum || R < 1 || C < 1 || ld_in < C || ld_out < R) return fail(SS_ERR_INVALID, "bad arguments");
+  return transpose_launch(in, ld_in, R, C, out, ld_out, colsum, stream);
 }
 
 int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream) {

@@ -252,11 +252,11 @@ class ProposalNet:
             M = self.B * (ho * wo if L.kind != 'fc' else 1)
             x = self.x0 if i == 0 else self.y[i - 1]
             dp = self.dpre[i]
-            _lib.check(self.L.ss_bias_grad_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self._view(self.grads, L.name + '.b')),
-                                                self._stream()), 'ss_bias_grad_bf16')
             M8 = round8(M)
-            _lib.check(self.L.ss_transpose_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self.dpret), M8, self._stream()),
-                       'ss_transpose_bf16')
+            # the transposed pre-activation gradient for the weight gradient, and the bias gradient, in one pass
+            _lib.check(self.L.ss_transpose_sum_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self.dpret), M8,
+                                                    _lib.ptr(self._view(self.grads, L.name + '.b')), self._stream()),
+                       'ss_transpose_sum_bf16')
             src, lds = (self.cols[i], Kc) if L.kind == 'conv' else (x, K)   # forward columns, or the input itself
             _lib.check(self.L.ss_transpose_bf16(_lib.ptr(src), lds, M, K, _lib.ptr(self.colst), M8, self._stream()),
                        'ss_transpose_bf16')
