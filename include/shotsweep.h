@@ -93,6 +93,11 @@ size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mod
  * drop-in's imaging_memory_bytes (openfwi/physics/gpu.py:70-73). */
 size_t ss_workspace_bytes_slots(const ss_geometry* geom, int32_t mode, int32_t slots);
 
+/* The inverse: how many solves a workspace of `bytes` keeps in flight (0:
+ * not even one; the plan's co-resident clusters cap it at launch).  Needs no
+ * device. */
+int32_t ss_workspace_slots(const ss_geometry* geom, int32_t mode, size_t bytes);
+
 /* Reads the device-side status word of `workspace` after synchronising
  * `stream`: SS_OK, SS_ERR_TIMEOUT if a bounded wait ran out, or
  * SS_ERR_NONFINITE if the observed gathers held a non-finite sample (the

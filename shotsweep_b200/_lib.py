@@ -80,6 +80,7 @@ _SIGNATURES = {
     'ss_last_error': (ctypes.c_char_p, []),
     'ss_workspace_bytes': (ctypes.c_size_t, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32]),
     'ss_set_rows_per_thread': (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32]),
+    'ss_workspace_slots': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_size_t]),
     'ss_workspace_bytes_slots': (ctypes.c_size_t, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32]),
     'ss_workspace_status': (ctypes.c_int32, [_P, _P]),
     'ss_plan_info': (ctypes.c_int32, [ctypes.POINTER(Geometry), ctypes.c_int32, ctypes.c_int32,

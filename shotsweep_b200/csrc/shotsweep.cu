@@ -1521,17 +1521,23 @@ WsLayout ws_layout(const ss_geometry* g, const Plan& p, int mode, int hist_steps
 }
 
 // The most solves in flight whose scratch fits `bytes` (0: not even one).
+// The layout grows monotonically with the slots (each region is 256-byte
+// aligned, so the growth per slot varies by a few bytes): binary search.
 int slots_for_bytes(const ss_geometry* g, Plan p, int mode, size_t bytes) {
-  p.slots = 1;
-  if (ws_layout(g, p, mode).total > bytes) return 0;
-  const size_t one = ws_layout(g, p, mode).total;
-  p.slots = 2;
-  const size_t per_slot = ws_layout(g, p, mode).total - one;   // alignment padding included
-  if (per_slot == 0) return 1 << 30;                          // forward mode: no per-slot scratch
-  int n = static_cast<int>(std::min<size_t>((bytes - one) / per_slot + 1, size_t(1) << 30));
-  p.slots = n;
-  while (n > 1 && ws_layout(g, p, mode).total > bytes) p.slots = --n;
-  return n;
+  auto total = [&](int n) {
+    p.slots = n;
+    return ws_layout(g, p, mode).total;
+  };
+  if (total(1) > bytes) return 0;
+  constexpr int kCap = 1 << 24;
+  if (total(kCap) <= bytes) return kCap;   // forward mode: no per-slot scratch
+  int lo = 1, hi = kCap;                    // total(lo) <= bytes < total(hi)
+  while (hi - lo > 1) {
+    const int mid = lo + (hi - lo) / 2;
+    if (total(mid) <= bytes) lo = mid;
+    else hi = mid;
+  }
+  return lo;
 }
 
 KParams base_params(const ss_geometry* g, const Plan& p, int n_models) {
@@ -2162,6 +2168,13 @@ size_t ss_workspace_bytes(const ss_geometry* geom, int32_t n_models, int32_t mod
   Plan p;
   if (make_plan(geom, mode, n_models * geom->n_shots, &p)) return 0;
   return ws_layout(geom, p, mode).total;
+}
+
+int32_t ss_workspace_slots(const ss_geometry* geom, int32_t mode, size_t bytes) {
+  if (check_geometry(geom) || mode < 0 || mode > 2) return 0;
+  Plan p;
+  if (plan_shape(geom, mode, &p)) return 0;
+  return slots_for_bytes(geom, p, mode, bytes);
 }
 
 int32_t ss_set_rows_per_thread(int32_t mode, int32_t rows) {

@@ -138,6 +138,19 @@ def test_workspace_per_slot_is_linear(lib):
     assert lib.ss_workspace_bytes_slots(ctypes.byref(g), _lib.MODE_FORWARD, 45) == 256
 
 
+def test_workspace_size_gives_back_its_solves_in_flight(lib):
+    """A workspace sized for k solves runs k at once, one byte less runs k - 1 (the regions' 256-byte
+    alignment makes the growth per solve uneven, so this is exact arithmetic, not a division)."""
+    import ctypes
+    from shotsweep_b200 import _lib, engine
+    for g in (engine.geometry(), engine.geometry(23, 37, 160, 9, (0, 18, 36))):
+        for mode in (_lib.MODE_GRADIENT, _lib.MODE_IMAGES):
+            for k in (1, 2, 3, 7, 44, 45, 46, 200, 4096):
+                b = lib.ss_workspace_bytes_slots(ctypes.byref(g), mode, k)
+                assert lib.ss_workspace_slots(ctypes.byref(g), mode, b) == k
+                assert lib.ss_workspace_slots(ctypes.byref(g), mode, b - 1) == k - 1
+
+
 def test_host_pipeline_chunks_cover_rows_in_whole_rounds():
     """The host-observation pipeline's chunks: contiguous, covering every row once, whole rounds of the
     persistent clusters except the last, growing x6 from one round, capped at a third of the rows and 1 GiB."""
