@@ -309,6 +309,46 @@ __global__ void im2col_t_kernel(const bf16* __restrict__ x, ConvGeom g, int K, i
   }
 }
 
+// Columns of small-K layers (K <= 64, Kc % 8 == 0; the first encoder layer,
+// whose 5 input channels rule out 16-byte gathers): each thread gathers one
+// pixel's row, tap by tap (runs of Cin contiguous inputs), into shared memory;
+// the CTA then writes its 256 consecutive rows with coalesced 16-byte stores.
+constexpr int kRowThreads = 256;
+__global__ void __launch_bounds__(kRowThreads) im2col_rows_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int Kc,
+                                                                  bf16* __restrict__ cols) {
+  extern __shared__ __align__(16) unsigned char rows_raw[];
+  bf16* rows = reinterpret_cast<bf16*>(rows_raw);   // [kRowThreads][Kc]
+  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
+  for (int64_t m0 = static_cast<int64_t>(blockIdx.x) * kRowThreads; m0 < M;
+       m0 += static_cast<int64_t>(gridDim.x) * kRowThreads) {
+    const int64_t m = m0 + threadIdx.x;
+    bf16* row = rows + threadIdx.x * Kc;
+    if (m < M) {
+      const int ox = static_cast<int>(m % g.Wout);
+      const int64_t t = m / g.Wout;
+      const int oy = static_cast<int>(t % g.Hout);
+      const int b = static_cast<int>(t / g.Hout);
+      for (int kh = 0; kh < g.KH; ++kh)
+        for (int kw = 0; kw < g.KW; ++kw) {
+          const int uy = oy * g.sh - g.ph + kh, ux = ox * g.sw - g.pw + kw;
+          const bool in = uy >= 0 && ux >= 0 && uy < g.Hin * g.up && ux < g.Win * g.up;
+          const bf16* src = in ? x + ((static_cast<int64_t>(b) * g.Hin + uy / g.up) * g.Win + ux / g.up) * g.Cin : x;
+          bf16* dst = row + (kh * g.KW + kw) * g.Cin;
+          for (int c = 0; c < g.Cin; ++c) dst[c] = in ? src[c] : __float2bfloat16_rn(0.f);
+        }
+      for (int k = K; k < Kc; ++k) row[k] = __float2bfloat16_rn(0.f);
+    }
+    __syncthreads();
+    const int64_t n_rows = M - m0 < kRowThreads ? M - m0 : static_cast<int64_t>(kRowThreads);
+    const int64_t n16 = n_rows * Kc / 8;   // 16-byte words of this CTA's rows
+    uint4* out = reinterpret_cast<uint4*>(cols + m0 * Kc);
+    const uint4* in16 = reinterpret_cast<const uint4*>(rows);
+    for (int64_t i = threadIdx.x; i < n16; i += kRowThreads) out[i] = in16[i];
+    __syncthreads();
+  }
+}
+
+
 // 4 channels per thread (Cin % 4 == 0 and a row stride Kc % 4 == 0): float4 gathers.
 __global__ void col2im_lrelu_vec4_kernel(const float* __restrict__ dcols, ConvGeom g, int Kc, const bf16* __restrict__ y,
                                          float slope, bf16* __restrict__ dpre, int64_t ldp) {
@@ -588,6 +628,157 @@ __global__ void head_dgrad_kernel(const bf16* __restrict__ x, HeadGeom g, const 
   }
 }
 
+// Output head with 8-channel (16-byte) input loads and the 3 x 3 x C weights
+// in shared memory; one thread per output pixel (C % 8 == 0, C <= 64).
+__global__ void __launch_bounds__(256) head_forward_v8_kernel(const bf16* __restrict__ x, HeadGeom g,
+                                                              const float* __restrict__ w,
+                                                              const float* __restrict__ bias_dev,
+                                                              float* __restrict__ out) {
+  __shared__ float ws[9 * 64];
+  for (int i = threadIdx.x; i < 9 * g.C; i += blockDim.x) ws[i] = w[i];
+  __syncthreads();
+  const float bias = *bias_dev;
+  const int64_t total = static_cast<int64_t>(g.B) * g.n * g.n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int xo = static_cast<int>(i % g.n), yo = static_cast<int>((i / g.n) % g.n);
+    const int b = static_cast<int>(i / (static_cast<int64_t>(g.n) * g.n));
+    float acc = bias;
+    for (int kh = 0; kh < 3; ++kh) {
+      const int yy = yo + kh - 1;
+      if (yy < 0 || yy >= g.n) continue;
+      for (int kw = 0; kw < 3; ++kw) {
+        const int xx = xo + kw - 1;
+        if (xx < 0 || xx >= g.n) continue;
+        const uint4* px =
+            reinterpret_cast<const uint4*>(x + ((static_cast<int64_t>(b) * g.H + yy + g.off) * g.W + xx + g.off) * g.C);
+        const float* wk = ws + (kh * 3 + kw) * g.C;
+        for (int q = 0; q < g.C / 8; ++q) {
+          const uint4 v = px[q];
+          const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float2 f = __bfloat1622float2(h[j]);
+            acc = fmaf(f.x, wk[8 * q + 2 * j], acc);
+            acc = fmaf(f.y, wk[8 * q + 2 * j + 1], acc);
+          }
+        }
+      }
+    }
+    out[i] = tanhf(acc);
+  }
+}
+
+// Head weight and bias gradients: dw[tap][c] = sum_p dpre[p] x[p + tap][c],
+// db = sum_p dpre[p].  Thread (pixel lane, 8-channel group) accumulates the
+// 9 x 8 products of its pixels in registers; lanes reduce with shuffles, warps
+// through shared memory, and each CTA adds its 9 x C sums with one atomic each.
+template <int CG>   // channel groups of 8: C = 8 * CG
+__global__ void __launch_bounds__(256) head_wgrad_v8_kernel(const bf16* __restrict__ x, HeadGeom g,
+                                                            const float* __restrict__ dpre, float* __restrict__ dw,
+                                                            float* __restrict__ db) {
+  constexpr int kLanes = 256 / CG;   // pixel lanes per CTA
+  __shared__ float red[8][CG][72];
+  __shared__ float redb[8];
+  const int cg = threadIdx.x % CG, pl = threadIdx.x / CG;
+  const int total = g.B * g.n * g.n;   // checked < 2^31 on the host
+  const int per = (total + gridDim.x - 1) / gridDim.x;
+  const int p0 = blockIdx.x * per, p1 = min(p0 + per, total);
+  float acc[72];
+#pragma unroll
+  for (int j = 0; j < 72; ++j) acc[j] = 0.f;
+  float accb = 0.f;
+  for (int p = p0 + pl; p < p1; p += kLanes) {
+    const float d = dpre[p];
+    accb += d;
+    const int xo = p % g.n, yo = (p / g.n) % g.n, b = p / (g.n * g.n);
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+      const int yy = yo + tap / 3 - 1, xx = xo + tap % 3 - 1;
+      if (yy < 0 || yy >= g.n || xx < 0 || xx >= g.n) continue;
+      const uint4 v = *reinterpret_cast<const uint4*>(
+          x + ((static_cast<int64_t>(b) * g.H + yy + g.off) * g.W + xx + g.off) * g.C + 8 * cg);
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float2 f = __bfloat1622float2(h[j]);
+        acc[tap * 8 + 2 * j] = fmaf(d, f.x, acc[tap * 8 + 2 * j]);
+        acc[tap * 8 + 2 * j + 1] = fmaf(d, f.y, acc[tap * 8 + 2 * j + 1]);
+      }
+    }
+  }
+  // lanes of one channel group within a warp: reduce over pixel lanes
+#pragma unroll
+  for (int j = 0; j < 72; ++j)
+    for (int o = CG; o < 32; o <<= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+  for (int o = 1; o < 32; o <<= 1) accb += __shfl_xor_sync(0xffffffffu, accb, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane < CG)
+#pragma unroll
+    for (int j = 0; j < 72; ++j) red[warp][lane][j] = acc[j];
+  if (lane == 0) redb[warp] = accb / CG;   // every channel group added the same dpre values
+  __syncthreads();
+  for (int o = threadIdx.x; o < 9 * 8 * CG; o += blockDim.x) {
+    const int tap = o / (8 * CG), c = o % (8 * CG);
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += red[k][c / 8][tap * 8 + c % 8];
+    atomicAdd(dw + o, s);
+  }
+  if (threadIdx.x == 0) {
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) s += redb[k];
+    atomicAdd(db, s);
+  }
+}
+
+// Head input gradient times the leaky-ReLU derivative of x, 8 channels per
+// thread (16-byte loads and stores), weights in shared memory.
+__global__ void __launch_bounds__(256) head_dgrad_v8_kernel(const bf16* __restrict__ x, HeadGeom g,
+                                                            const float* __restrict__ dpre,
+                                                            const float* __restrict__ w, float slope,
+                                                            bf16* __restrict__ dpre_x) {
+  __shared__ float ws[9 * 64];
+  for (int i = threadIdx.x; i < 9 * g.C; i += blockDim.x) ws[i] = w[i];
+  __syncthreads();
+  const int cgs = g.C / 8;
+  const int64_t total = static_cast<int64_t>(g.B) * g.H * g.W * cgs;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c0 = static_cast<int>(i % cgs) * 8;
+    const int64_t pix = i / cgs;
+    const int X = static_cast<int>(pix % g.W), Y = static_cast<int>((pix / g.W) % g.H);
+    const int b = static_cast<int>(pix / (static_cast<int64_t>(g.W) * g.H));
+    const int yy = Y - g.off, xx = X - g.off;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (yy >= 0 && yy < g.n && xx >= 0 && xx < g.n)
+      for (int kh = 0; kh < 3; ++kh) {
+        const int yo = yy - kh + 1;
+        if (yo < 0 || yo >= g.n) continue;
+        for (int kw = 0; kw < 3; ++kw) {
+          const int xo = xx - kw + 1;
+          if (xo < 0 || xo >= g.n) continue;
+          const float d = dpre[(static_cast<int64_t>(b) * g.n + yo) * g.n + xo];
+          const float* wk = ws + (kh * 3 + kw) * g.C + c0;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[j] = fmaf(d, wk[j], acc[j]);
+        }
+      }
+    const uint4 yv = *reinterpret_cast<const uint4*>(x + pix * g.C + c0);
+    const __nv_bfloat162* yh = reinterpret_cast<const __nv_bfloat162*>(&yv);
+    uint4 o;
+    __nv_bfloat162* oh = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float2 f = __bfloat1622float2(yh[j]);
+      const float a0 = f.x > 0.f ? acc[2 * j] : slope * acc[2 * j];
+      const float a1 = f.y > 0.f ? acc[2 * j + 1] : slope * acc[2 * j + 1];
+      oh[j] = __floats2bfloat162_rn(a0, a1);
+    }
+    *reinterpret_cast<uint4*>(dpre_x + pix * g.C + c0) = o;
+  }
+}
+
 // AdamW (decoupled weight decay), then the BF16 copy used by the GEMMs.
 __global__ void step_inc_kernel(int* step) { *step += 1; }
 
@@ -706,6 +897,10 @@ int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t t
   else if (g.Cin % 8 == 0 && Kc == K && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
            (reinterpret_cast<uintptr_t>(cols) & 15) == 0)
     im2col_vec8_kernel<<<grid_for_l(M * K / 8), 256, 0, st>>>(static_cast<const bf16*>(x), g, static_cast<bf16*>(cols));
+  else if (Kc % 8 == 0 && Kc <= 96 && (reinterpret_cast<uintptr_t>(cols) & 15) == 0)
+    im2col_rows_kernel<<<static_cast<int>(std::min<long long>((M + kRowThreads - 1) / kRowThreads, 148LL * 8)),
+                         kRowThreads, kRowThreads * Kc * sizeof(bf16), st>>>(static_cast<const bf16*>(x), g, K, Kc,
+                                                                             static_cast<bf16*>(cols));
   else
     im2col_kernel<<<grid_for_l(M * Kc), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, Kc, static_cast<bf16*>(cols));
   SS_TRY_CUDA(cudaGetLastError());
@@ -782,6 +977,11 @@ int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, fl
   return SS_OK;
 }
 
+// The 16-byte head kernels: channels a multiple of 8 (at most 64), 16-byte aligned map.
+static bool head_v8_ok(const void* x, const HeadGeom& g) {
+  return g.C % 8 == 0 && g.C <= 64 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+}
+
 // head: {B, H, W, C, off, n}
 int32_t ss_head_forward(const void* x, const int32_t* head, const float* w, const float* bias, float* out, void* stream) {
   ss_internal::clear_error();
@@ -789,8 +989,12 @@ int32_t ss_head_forward(const void* x, const int32_t* head, const float* w, cons
   const HeadGeom g{head[0], head[1], head[2], head[3], head[4], head[5]};
   if (g.off < 0 || g.off + g.n > g.H || g.off + g.n > g.W) return fail(SS_ERR_INVALID, "crop outside the map");
   const long long total = static_cast<long long>(g.B) * g.n * g.n;
-  head_forward_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(x), g,
-                                                                                       w, bias, out);
+  if (head_v8_ok(x, g))
+    head_forward_v8_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(x), g, w, bias, out);
+  else
+    head_forward_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(x),
+                                                                                         g, w, bias, out);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }
@@ -803,10 +1007,16 @@ int32_t ss_head_backward(const void* x, const int32_t* head, const float* w, con
   if (9 * g.C > 1024) return fail(SS_ERR_UNSUPPORTED, "head with more than 113 channels");
   if (static_cast<long long>(g.B) * g.n * g.n >= (1LL << 31)) return fail(SS_ERR_UNSUPPORTED, "head output beyond 2^31 values");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  head_wgrad_kernel<<<296, 9 * g.C, 0, st>>>(static_cast<const bf16*>(x), g, dpre, dw, db);
   const long long total = static_cast<long long>(g.B) * g.H * g.W * g.C;
-  head_dgrad_kernel<<<grid_for_l(total), 256, 0, st>>>(static_cast<const bf16*>(x), g, dpre, w, slope,
-                                                        static_cast<bf16*>(dpre_x));
+  if (head_v8_ok(x, g) && (reinterpret_cast<uintptr_t>(dpre_x) & 15) == 0 && g.C == 32) {
+    head_wgrad_v8_kernel<4><<<592, 256, 0, st>>>(static_cast<const bf16*>(x), g, dpre, dw, db);
+    head_dgrad_v8_kernel<<<grid_for_l(total / 8), 256, 0, st>>>(static_cast<const bf16*>(x), g, dpre, w, slope,
+                                                                 static_cast<bf16*>(dpre_x));
+  } else {
+    head_wgrad_kernel<<<296, 9 * g.C, 0, st>>>(static_cast<const bf16*>(x), g, dpre, dw, db);
+    head_dgrad_kernel<<<grid_for_l(total), 256, 0, st>>>(static_cast<const bf16*>(x), g, dpre, w, slope,
+                                                          static_cast<bf16*>(dpre_x));
+  }
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }

@@ -429,7 +429,7 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
           }
 
 // Body of one tile row k (a compile-time constant after unrolling) inside
-// solve_kernel's step; written once, expanded in two row orders, each with
+// solve_kernel's step; written once, expanded with
 // (SPECIAL) and without the source / receiver terms.  The row's two x-halo
 // pairs lf / rt come from the enclosing loop, which loads them one row ahead
 // (1.2 % faster than loading them at the row).
@@ -690,10 +690,6 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
     const uint32_t dn_bar = edge_dn ? mapa(halo_bar0, rank + 1) : 0u;
     const uint32_t halo_bytes = 32u * GNCG * ((rank > 0 ? 1u : 0u) + (rank < P.C - 1 ? 1u : 0u));
     const int rec_k = (active && src_r >= myrow && src_r < myrow + H) ? src_r - myrow : -1;
-    // A warp with any tile on the lower band edge computes its rows bottom-up,
-    // so that the rows pushed to the next band are ready early in the step;
-    // the order is uniform per warp (the tile is in registers, any order works).
-    const bool rev_rows = __ballot_sync(0xffffffffu, edge_dn) != 0u;
     // Warp-uniform forms of per-thread conditions of the step (votes, which
     // the compiler knows are uniform): the branches they guard need no
     // reconvergence in the warps that skip them.
@@ -856,10 +852,12 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
                                   : nullptr;
         const float* hl = fwd ? nullptr : (active ? stage_buf(bi) + lr0 * SW + 4 * cg : dstg);
         auto as4 = [](const float2(&r)[2]) { return make_float4(r[0].x, r[0].y, r[1].x, r[1].y); };
-        // Threads on the lower band edge compute their bottom rows first, so
-        // that the halo push to the next band leaves early in the step.  The
-        // source and receiver terms are compiled into the rows of the first
-        // branch only (one warp-uniform branch per step instead of one per row).
+        // Every warp computes its rows top-down (a second, bottom-up copy of the
+        // row loop for the warps on the lower band edge, so that their halo push
+        // left earlier, measured 3.1 % slower: the doubled step code missed the
+        // instruction cache).  The source and receiver terms are compiled into
+        // the rows of the first branch only (one warp-uniform branch per step
+        // instead of one per row).
         // Adjoint, receiver warps: this step's residual at the tile's four
         // columns (zero off the receiver columns), read once for all rows.
         // Forward: this step's source amount at each of the tile's columns.
@@ -880,21 +878,7 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
             rv2 = (rr + 2 >= 0 && rr + 2 < NX) ? rs[min(max(rr + 2, 0), NX - 1)] : 0.f;
             rv3 = (rr + 3 >= 0 && rr + 3 < NX) ? rs[min(max(rr + 3, 0), NX - 1)] : 0.f;
           }
-          if (rev_rows) {
-            float2 lfn = *reinterpret_cast<const float2*>(xc + (H + 1) * RS - 2);
-            float2 rtn = *reinterpret_cast<const float2*>(xc + (H + 1) * RS + 4);
-#pragma unroll
-            for (int i = 0; i < H; ++i) {
-              const int k = H - 1 - i;
-              const float2 lf = lfn, rt = rtn;
-              if (i + 1 < H) {
-                lfn = *reinterpret_cast<const float2*>(xc + (k + 1) * RS - 2);
-                rtn = *reinterpret_cast<const float2*>(xc + (k + 1) * RS + 4);
-              }
-              SS_COEF_ROW(k)
-              SS_TILE_ROW(k, true)
-            }
-          } else {
+          {
             float2 lfn = *reinterpret_cast<const float2*>(xc + 2 * RS - 2);
             float2 rtn = *reinterpret_cast<const float2*>(xc + 2 * RS + 4);
 #pragma unroll
@@ -909,21 +893,7 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
             }
           }
         } else {
-          if (rev_rows) {
-            float2 lfn = *reinterpret_cast<const float2*>(xc + (H + 1) * RS - 2);
-            float2 rtn = *reinterpret_cast<const float2*>(xc + (H + 1) * RS + 4);
-#pragma unroll
-            for (int i = 0; i < H; ++i) {
-              const int k = H - 1 - i;
-              const float2 lf = lfn, rt = rtn;
-              if (i + 1 < H) {
-                lfn = *reinterpret_cast<const float2*>(xc + (k + 1) * RS - 2);
-                rtn = *reinterpret_cast<const float2*>(xc + (k + 1) * RS + 4);
-              }
-              SS_COEF_ROW(k)
-              SS_TILE_ROW(k, false)
-            }
-          } else {
+          {
             float2 lfn = *reinterpret_cast<const float2*>(xc + 2 * RS - 2);
             float2 rtn = *reinterpret_cast<const float2*>(xc + 2 * RS + 4);
 #pragma unroll
