@@ -451,24 +451,31 @@ __global__ void transpose_bf16_kernel(const bf16* __restrict__ in, int64_t ld_in
 }
 
 // out[c][r] = in[r][c] for a [R][C] BF16 matrix (row strides ld_in, ld_out, both
-// even), in 64 x 64 tiles: rows are read and written as BF16 pairs (4-byte
-// accesses), staged in shared memory.  With colsum != NULL the block also adds
-// the column sums of its rows into colsum (float), one atomic per column per
-// block: a CTA walks `tiles` row tiles so that the atomics stay few.
+// even), in tiles of 64 rows x TW columns (TW = 64, or 32 for matrices of at
+// most 32 columns, so that narrow matrices keep every thread busy): rows are
+// read and written as BF16 pairs (4-byte accesses), staged in shared memory.
+// With colsum != NULL the CTA also adds the column sums of its rows into
+// colsum (float), one atomic per column per CTA: a CTA walks `tiles` row
+// tiles so that the atomics stay few.
 constexpr int kTT = 64;
+template <int TW>
 __global__ void __launch_bounds__(256) transpose_sum_kernel(const bf16* __restrict__ in, int64_t ld_in, int R, int C,
                                                             bf16* __restrict__ out, int64_t ld_out,
                                                             float* __restrict__ colsum, int tiles) {
-  __shared__ bf16 tile[kTT][kTT + 2];
-  __shared__ float part[8][kTT];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int c0 = blockIdx.x * kTT;
+  constexpr int kPairs = TW / 2;              // threads per tile row when loading
+  constexpr int kRowsPass = 256 / kPairs;     // tile rows loaded per pass
+  __shared__ bf16 tile[kTT][TW + 2];
+  __shared__ float part[kRowsPass][TW];
+  const int tx = threadIdx.x % kPairs, ty = threadIdx.x / kPairs;
+  const int wx = threadIdx.x & 31, wy = threadIdx.x >> 5;   // store phase: 32 pairs of rows per column
+  const int c0 = blockIdx.x * TW;
   const int c = c0 + 2 * tx;
   float s0 = 0.f, s1 = 0.f;
   for (int t = 0; t < tiles; ++t) {
     const int64_t r0 = (static_cast<int64_t>(blockIdx.y) * tiles + t) * kTT;
     if (r0 >= R) break;
-    for (int j = ty; j < kTT; j += 8) {
+#pragma unroll
+    for (int j = ty; j < kTT; j += kRowsPass) {
       const int64_t r = r0 + j;
       bf16 a = __float2bfloat16(0.f), b = a;
       if (r < R) {
@@ -487,18 +494,19 @@ __global__ void __launch_bounds__(256) transpose_sum_kernel(const bf16* __restri
       s1 += __bfloat162float(b);
     }
     __syncthreads();
-    for (int j = ty; j < kTT; j += 8) {
+#pragma unroll
+    for (int j = wy; j < TW; j += 8) {
       const int cc = c0 + j;
-      const int64_t r = r0 + 2 * tx;
+      const int64_t r = r0 + 2 * wx;
       if (cc < C && r < R) {
         bf16* q = out + static_cast<int64_t>(cc) * ld_out + r;
         if (r + 1 < R) {
           __nv_bfloat162 v;
-          v.x = tile[2 * tx][j];
-          v.y = tile[2 * tx + 1][j];
+          v.x = tile[2 * wx][j];
+          v.y = tile[2 * wx + 1][j];
           *reinterpret_cast<__nv_bfloat162*>(q) = v;
         } else {
-          q[0] = tile[2 * tx][j];
+          q[0] = tile[2 * wx][j];
         }
       }
     }
@@ -508,10 +516,10 @@ __global__ void __launch_bounds__(256) transpose_sum_kernel(const bf16* __restri
     part[ty][2 * tx] = s0;
     part[ty][2 * tx + 1] = s1;
     __syncthreads();
-    if (threadIdx.x < kTT && c0 + threadIdx.x < C) {
+    if (threadIdx.x < TW && c0 + threadIdx.x < C) {
       float s = 0.f;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) s += part[k][threadIdx.x];
+      for (int k = 0; k < kRowsPass; ++k) s += part[k][threadIdx.x];
       atomicAdd(colsum + c0 + threadIdx.x, s);
     }
   }
@@ -934,14 +942,20 @@ static int transpose_launch(const void* in, int64_t ld_in, int32_t R, int32_t C,
   const bool pairs = (ld_in % 2 == 0) && (ld_out % 2 == 0) && (reinterpret_cast<uintptr_t>(in) % 4 == 0) &&
                      (reinterpret_cast<uintptr_t>(out) % 4 == 0);
   if (pairs) {
-    const int gx = (C + kTT - 1) / kTT;
+    const int tw = C <= 32 ? 32 : 64;
+    const int gx = (C + tw - 1) / tw;
     const long long row_tiles = (static_cast<long long>(R) + kTT - 1) / kTT;
-    // with column sums, enough row tiles per CTA that about 4 CTAs per SM remain (few atomics per column)
-    const int tiles = colsum ? static_cast<int>(std::max<long long>(1, row_tiles * gx / 592)) : 1;
+    // with column sums, enough row tiles per CTA that about 8 CTAs per SM remain (few atomics per column)
+    const int tiles = colsum ? static_cast<int>(std::max<long long>(1, row_tiles * gx / (148 * 8))) : 1;
     const long long gy = (row_tiles + tiles - 1) / tiles;
     if (gy > 65535) return fail(SS_ERR_UNSUPPORTED, "matrix too tall to transpose");
-    transpose_sum_kernel<<<dim3(gx, static_cast<unsigned>(gy)), 256, 0, st>>>(
-        static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out), ld_out, colsum, tiles);
+    const dim3 grid(gx, static_cast<unsigned>(gy));
+    if (tw == 32)
+      transpose_sum_kernel<32><<<grid, 256, 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out),
+                                                     ld_out, colsum, tiles);
+    else
+      transpose_sum_kernel<64><<<grid, 256, 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out),
+                                                     ld_out, colsum, tiles);
   } else {
     dim3 grid((C + 31) / 32, (R + 31) / 32);
     transpose_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C,
