@@ -446,24 +446,22 @@ __device__ __forceinline__ void st_async_v4_if(bool p, uint32_t addr, float4 v, 
           float4 nw = make_float4(n_lo.x, n_lo.y, n_hi.x, n_hi.y); \
           if (fwd) { \
             if (SPECIAL) {  /* injection after damping (gpu.py:113-114): + w at the source cell */ \
-              const float on = (k == src_k) ? 1.f : 0.f; \
-              nw.x = fmaf(on, am0, nw.x); \
-              nw.y = fmaf(on, am1, nw.y); \
-              nw.z = fmaf(on, am2, nw.z); \
-              nw.w = fmaf(on, am3, nw.w); \
+              if (k == src_k) { \
+                nw.x = fmaf(1.f, am0, nw.x); \
+                nw.y = fmaf(1.f, am1, nw.y); \
+                nw.z = fmaf(1.f, am2, nw.z); \
+                nw.w = fmaf(1.f, am3, nw.w); \
+              } \
             } \
           } else { \
-            if (SPECIAL) {  /* residual injection th += sigma*res (gpu.py:180), res loaded once per step */ \
-              const bool on = k == rec_k; \
-              nw.x = fmaf(on ? -cs0.x : 0.f, rv0, nw.x); \
-              nw.y = fmaf(on ? -cs0.y : 0.f, rv1, nw.y); \
-              nw.z = fmaf(on ? -cs1.x : 0.f, rv2, nw.z); \
-              nw.w = fmaf(on ? -cs1.y : 0.f, rv3, nw.w); \
-            } \
-            if (SPECIAL) {  /* source-strength term (gpu.py:182) */ \
-              const float a = (k == src_k) ? wt : 0.f; \
-              const float q = src_m == 0 ? nw.x : src_m == 1 ? nw.y : src_m == 2 ? nw.z : nw.w; \
-              src_acc = fmaf(q, a, src_acc); \
+            if (SPECIAL) {  /* residual injection th += sigma*res (gpu.py:180), res loaded once per step; */ \
+              /* a branch on the one receiver row (per-row selects on every row measured 1.3 % slower) */ \
+              if (k == rec_k) { \
+                nw.x = fmaf(-cs0.x, rv0, nw.x); \
+                nw.y = fmaf(-cs0.y, rv1, nw.y); \
+                nw.z = fmaf(-cs1.x, rv2, nw.z); \
+                nw.w = fmaf(-cs1.y, rv3, nw.w); \
+              } \
             } \
           } \
           if (k < 2) \
@@ -892,6 +890,11 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
               SS_TILE_ROW(k, true)
             }
           }
+          // Adjoint: source-strength term (gpu.py:182) from the source cell's new
+          // value, read back from the field this thread just wrote, once per step
+          // (in the row loop it cost every row of the receiver warps, which pace
+          // the cluster).
+          if (!fwd && src_k >= 0) src_acc = fmaf(yc[src_k * RS + src_m], wt, src_acc);
         } else {
           {
             float2 lfn = *reinterpret_cast<const float2*>(xc + 2 * RS - 2);
