@@ -414,6 +414,9 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
  *   ss_col2im_lrelu_bf16  dpre[pixel][c] (row stride ldp) = leaky_relu'(y) x the
  *                         sum of the column gradients dcols [pixels_out][Kc]
  *                         that read input element (pixel, c); y: the input map
+ *   ss_im2col_both_bf16   cols [pixels][Kc] and, in the same pass, the columns
+ *                         transposed [Kc][ldt] (Cin % 8 == 0, Kc == K): the
+ *                         forward GEMM's operand and the weight gradient's
  *   ss_transpose_bf16     out[c][r] = in[r][c]
  *   ss_transpose_sum_bf16 the same, and colsum[c] += sum over rows of in[r][c]
  *                         in the same pass (a layer's bias gradient from its
@@ -432,6 +435,8 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
  *                         samples ids[0..B) as BF16 [B][T][X][S] / scale (3_train.py:198) */
 int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t transposed, int64_t ldt, void* cols,
                        void* stream);
+int32_t ss_im2col_both_bf16(const void* x, const int32_t* conv, int32_t Kc, void* cols, void* colst, int64_t ldt,
+                            void* stream);
 int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
                              void* dpre, int64_t ldp, void* stream);
 int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream);

@@ -349,6 +349,55 @@ __global__ void __launch_bounds__(kRowThreads) im2col_rows_kernel(const bf16* __
 }
 
 
+// Columns and their transpose in one pass (Cin % 8 == 0, K == Kc): a CTA
+// gathers a tile of 64 pixels x 64 column indices from the input map with
+// 16-byte loads into shared memory, writes the columns row by row (cols
+// [pixels][K], the forward GEMM's operand) and the same tile transposed
+// (colst [K][ldt], pixels innermost, the weight-gradient GEMM's operand), so
+// that the backward pass needs no transpose of the columns.
+__global__ void __launch_bounds__(256) im2col_both_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int64_t ldt,
+                                                          bf16* __restrict__ cols, bf16* __restrict__ colst) {
+  __shared__ uint32_t tile[64][33];   // [pixel][pair of columns], padded against bank conflicts
+  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
+  const int k0 = blockIdx.x * 64;
+  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * 64;
+  const int c8 = threadIdx.x & 7, pl = threadIdx.x >> 3;   // 8-column chunk, pixel within the tile (0..31)
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int p = pl + 32 * h;
+    const int64_t m = m0 + p;
+    const int k = k0 + 8 * c8;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (m < M && k < K) {
+      const int64_t src = conv_src(g, m, k);
+      if (src >= 0) v = *reinterpret_cast<const uint4*>(x + src);
+      *reinterpret_cast<uint4*>(cols + m * K + k) = v;
+    }
+    tile[p][4 * c8 + 0] = v.x;
+    tile[p][4 * c8 + 1] = v.y;
+    tile[p][4 * c8 + 2] = v.z;
+    tile[p][4 * c8 + 3] = v.w;
+  }
+  __syncthreads();
+  // transposed: column index kk of the tile, pixels 2j and 2j+1 as one BF16 pair
+  const int j = threadIdx.x & 31, kr = threadIdx.x >> 5;
+  const int64_t m = m0 + 2 * j;
+#pragma unroll
+  for (int kk = kr; kk < 64; kk += 8) {
+    const int k = k0 + kk;
+    if (k >= K || m >= M) continue;
+    const uint32_t a = tile[2 * j][kk >> 1], b = tile[2 * j + 1][kk >> 1];
+    const uint16_t lo = (kk & 1) ? static_cast<uint16_t>(a >> 16) : static_cast<uint16_t>(a & 0xffffu);
+    const uint16_t hi = (kk & 1) ? static_cast<uint16_t>(b >> 16) : static_cast<uint16_t>(b & 0xffffu);
+    bf16* q = colst + static_cast<int64_t>(k) * ldt + m;
+    if (m + 1 < M) {
+      *reinterpret_cast<uint32_t*>(q) = static_cast<uint32_t>(lo) | (static_cast<uint32_t>(hi) << 16);
+    } else {
+      *reinterpret_cast<uint16_t*>(q) = lo;
+    }
+  }
+}
+
 // 4 channels per thread (Cin % 4 == 0 and a row stride Kc % 4 == 0): float4 gathers.
 __global__ void col2im_lrelu_vec4_kernel(const float* __restrict__ dcols, ConvGeom g, int Kc, const bf16* __restrict__ y,
                                          float slope, bf16* __restrict__ dpre, int64_t ldp) {
@@ -911,6 +960,26 @@ int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t t
                                                                              static_cast<bf16*>(cols));
   else
     im2col_kernel<<<grid_for_l(M * Kc), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, Kc, static_cast<bf16*>(cols));
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
+int32_t ss_im2col_both_bf16(const void* x, const int32_t* conv, int32_t Kc, void* cols, void* colst, int64_t ldt,
+                            void* stream) {
+  ss_internal::clear_error();
+  if (!x || !conv || !cols || !colst) return fail(SS_ERR_INVALID, "bad arguments");
+  const ConvGeom g = conv_geom(conv);
+  const int K = g.KH * g.KW * g.Cin;
+  if (g.Hout < 1 || g.Wout < 1 || g.up < 1 || g.sh < 1 || g.sw < 1) return fail(SS_ERR_INVALID, "bad convolution");
+  if (g.Cin % 8 != 0 || Kc != K || ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(cols)) & 15) != 0 ||
+      (reinterpret_cast<uintptr_t>(colst) & 3) != 0)
+    return fail(SS_ERR_UNSUPPORTED, "columns and transpose together need Cin % 8 == 0, Kc == K and aligned buffers");
+  const long long M = static_cast<long long>(g.B) * g.Hout * g.Wout;
+  if (ldt < M || (ldt & 1)) return fail(SS_ERR_INVALID, "transposed columns need an even ldt >= pixels");
+  const long long gy = (M + 63) / 64;
+  if (gy > 65535) return fail(SS_ERR_UNSUPPORTED, "too many pixels for one launch");
+  im2col_both_kernel<<<dim3((K + 63) / 64, static_cast<unsigned>(gy)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const bf16*>(x), g, K, ldt, static_cast<bf16*>(cols), static_cast<bf16*>(colst));
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }

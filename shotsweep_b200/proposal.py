@@ -153,12 +153,16 @@ class ProposalNet:
         self.x0 = torch.empty(B * T_IN * X_IN * S_IN, **bf)
         self.y = []
         self.cols = []       # each convolution's im2col columns, kept from forward to backward
+        self.colst_l = []    # and their transpose, written in the same pass where the channels allow
         max_colst = max_dcols = max_wt = max_dpret = 1
         for L, (hi, wi, ho, wo, K, Kc, N) in zip(LAYERS, self.shapes):
             M = B * (ho * wo if L.kind != 'fc' else 1)
             self.y.append(torch.empty(M * N, **bf))
             self.cols.append(torch.empty(M * Kc, **bf) if L.kind == 'conv' else None)
-            max_colst = max(max_colst, K * round8(M))
+            both = L.kind == 'conv' and L.cin % 8 == 0 and K == Kc
+            self.colst_l.append(torch.empty(K * round8(M), **bf) if both else None)
+            if not both:
+                max_colst = max(max_colst, K * round8(M))
             max_dcols = max(max_dcols, M * K)
             max_wt = max(max_wt, K * round8(N))
             max_dpret = max(max_dpret, N * round8(M))
@@ -221,8 +225,13 @@ class ProposalNet:
             hi, wi, ho, wo, K, Kc, N = self.shapes[i]
             M = self.B * (ho * wo if L.kind != 'fc' else 1)
             if L.kind == 'conv':
-                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols[i]),
-                                                 self._stream()), 'ss_im2col_bf16')
+                if self.colst_l[i] is not None:   # the columns and their transpose for the weight gradient
+                    _lib.check(self.L.ss_im2col_both_bf16(_lib.ptr(x), self._conv(i), Kc, _lib.ptr(self.cols[i]),
+                                                          _lib.ptr(self.colst_l[i]), round8(M), self._stream()),
+                               'ss_im2col_both_bf16')
+                else:
+                    _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols[i]),
+                                                     self._stream()), 'ss_im2col_bf16')
                 A, lda = self.cols[i], Kc
             else:
                 A, lda = x, K
@@ -257,10 +266,13 @@ class ProposalNet:
             _lib.check(self.L.ss_transpose_sum_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self.dpret), M8,
                                                     _lib.ptr(self._view(self.grads, L.name + '.b')), self._stream()),
                        'ss_transpose_sum_bf16')
-            src, lds = (self.cols[i], Kc) if L.kind == 'conv' else (x, K)   # forward columns, or the input itself
-            _lib.check(self.L.ss_transpose_bf16(_lib.ptr(src), lds, M, K, _lib.ptr(self.colst), M8, self._stream()),
-                       'ss_transpose_bf16')
-            self._gemm(self.dpret, M8, self.colst, M8, N, K, M, _lib.EPI_F32_ADD,
+            colst = self.colst_l[i]
+            if colst is None:
+                src, lds = (self.cols[i], Kc) if L.kind == 'conv' else (x, K)   # forward columns, or the input itself
+                _lib.check(self.L.ss_transpose_bf16(_lib.ptr(src), lds, M, K, _lib.ptr(self.colst), M8, self._stream()),
+                           'ss_transpose_bf16')
+                colst = self.colst
+            self._gemm(self.dpret, M8, colst, M8, N, K, M, _lib.EPI_F32_ADD,
                        self._view(self.grads, L.name + '.w'), Kc)
             if i == 0:
                 break
