@@ -43,11 +43,14 @@ struct GemmArgs {
   const float* bias;
   float slope;
   int* err;
+  int stages;   // ring slots in use (1..kStagesG): no more than the K steps of a CTA, so that short-K
+                // GEMMs take less shared memory and several CTAs share an SM (one's epilogue overlaps
+                // another's loads and MMAs)
 };
 
 template <int BN>
-constexpr size_t gemm_smem_bytes() {
-  return 1024 + kStagesG * (kBM * 128 + BN * 128) + (2 * kStagesG + 1) * 8 + 16;
+constexpr size_t gemm_smem_bytes(int stages = kStagesG) {
+  return 1024 + static_cast<size_t>(stages) * (kBM * 128 + BN * 128) + (2 * kStagesG + 1) * 8 + 16;
 }
 
 template <int BN, int EPI>
@@ -58,7 +61,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + kStagesG * STAGE);
+  const int ns = g.stages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + ns * STAGE);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2 * kStagesG + 1);
   const uint32_t sbase = smem_u32(base);
   auto full = [&](int s) { return smem_u32(&bars[s]); };
@@ -87,8 +91,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
   if (warp == 0 && lane == 0) {
     // ---- producer: A and B tiles of each K step into the ring ----------
     for (int i = 0; i < nk; ++i) {
-      const int s = i % kStagesG;
-      if (i >= kStagesG && !mbar_wait(empty(s), ((i / kStagesG) - 1) & 1, g.err, 1)) break;
+      const int s = i % ns;
+      if (i >= ns && !mbar_wait(empty(s), ((i / ns) - 1) & 1, g.err, 1)) break;
       mbar_expect_tx(full(s), STAGE);
       tma_load_2d(sbase + s * STAGE, &ta, (kt0 + i) * kBK, m0, full(s));
       tma_load_2d(sbase + s * STAGE + A_BYTES, &tb, (kt0 + i) * kBK, n0, full(s));
@@ -97,8 +101,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     // ---- MMA issuer: four K=16 MMAs per stage, the stage freed on completion
     constexpr uint32_t idesc = idesc_bf16_f32(kBM, BN);
     for (int i = 0; i < nk; ++i) {
-      const int s = i % kStagesG;
-      if (!mbar_wait(full(s), (i / kStagesG) & 1, g.err, 2)) break;
+      const int s = i % ns;
+      if (!mbar_wait(full(s), (i / ns) & 1, g.err, 2)) break;
       tc_fence_after();
       const uint64_t da = desc_sw128_kmajor(sbase + s * STAGE);
       const uint64_t db = desc_sw128_kmajor(sbase + s * STAGE + A_BYTES);
@@ -109,66 +113,71 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     mma_commit(acc_bar);
   } else if (warp >= 2) {
-    // ---- epilogue: warp w reads TMEM lanes 32*(w%4) .. +31, one row each --
+    // ---- epilogue: warp w owns TMEM lanes 32*(w%4) .. +31 (rows of the tile).
+    // Each 32-column slab goes TMEM -> registers (one row per thread) -> a
+    // padded 32 x 33 shared slab -> registers (8 threads per row, 4 columns
+    // each), so every store instruction covers 4 whole rows of 32 columns.
+    // The ring is free once the accumulator barrier completes (every load was
+    // consumed by an MMA that has finished), so the slabs live in stage 0.
     mbar_wait(acc_bar, 0, g.err, 3);
     tc_fence_after();
     const int q = warp & 3;
-    const int row = m0 + q * 32 + lane;
+    float* slab = reinterpret_cast<float*>(base) + q * (32 * 33);
+    const int rsub = lane >> 3, c4 = (lane & 7) * 4;
+    const bool vec = g.ldc % 4 == 0;
 #pragma unroll 1
-    for (int c = 0; c < BN; c += 16) {
-      float v[16];
-      tmem_ld16(taddr + (static_cast<uint32_t>(q * 32) << 16) + c, v);
-      if (row >= g.M) continue;
-      const long long off = static_cast<long long>(row) * g.ldc;
-      const int cbase = n0 + c;
-      // whole 16-column chunks with aligned rows: vector stores
-      if (cbase + 16 <= g.N && (EPI == SS_EPI_BIAS_LRELU_BF16 ? (g.ldc % 8 == 0) : (g.ldc % 4 == 0))) {
-        if (EPI == SS_EPI_BIAS_LRELU_BF16) {
-          __align__(16) bf16 o[16];
+    for (int c = 0; c < BN && n0 + c < g.N; c += 32) {
+      float v[32];
+      tmem_ld32(taddr + (static_cast<uint32_t>(q * 32) << 16) + c, v);
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            float x = v[j] + (g.bias ? g.bias[cbase + j] : 0.f);
-            o[j] = __float2bfloat16_rn(x > 0.f ? x : g.slope * x);
+      for (int j = 0; j < 32; ++j) slab[lane * 33 + j] = v[j];
+      __syncwarp();
+      const int col = n0 + c + c4;
+      float bj[4] = {0.f, 0.f, 0.f, 0.f};
+      if ((EPI == SS_EPI_BIAS_LRELU_BF16 || EPI == SS_EPI_BIAS_F32) && g.bias) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bj[j] = col + j < g.N ? g.bias[col + j] : 0.f;
+      }
+#pragma unroll
+      for (int pass = 0; pass < 8; ++pass) {
+        const int r = pass * 4 + rsub;
+        const int row = m0 + q * 32 + r;
+        float x[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          x[j] = slab[r * 33 + c4 + j] + bj[j];
+          if (EPI == SS_EPI_BIAS_LRELU_BF16) x[j] = x[j] > 0.f ? x[j] : g.slope * x[j];
+        }
+        if (row >= g.M) continue;
+        const long long off = static_cast<long long>(row) * g.ldc + col;
+        if (vec && col + 4 <= g.N) {
+          if (EPI == SS_EPI_BIAS_LRELU_BF16) {
+            __align__(8) bf16 o[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) o[j] = __float2bfloat16_rn(x[j]);
+            *reinterpret_cast<uint2*>(static_cast<bf16*>(g.c) + off) = *reinterpret_cast<const uint2*>(o);
+          } else {
+            float4* dst = reinterpret_cast<float4*>(static_cast<float*>(g.c) + off);
+            const float4 q4 = make_float4(x[0], x[1], x[2], x[3]);
+            if (EPI == SS_EPI_F32_ADD)
+              atomicAdd(dst, q4);
+            else
+              *dst = q4;
           }
-          uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(g.c) + off + cbase);
-          dst[0] = reinterpret_cast<const uint4*>(o)[0];
-          dst[1] = reinterpret_cast<const uint4*>(o)[1];
         } else {
-          float4* dst = reinterpret_cast<float4*>(static_cast<float*>(g.c) + off + cbase);
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            float4 q = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-            if (EPI == SS_EPI_BIAS_F32 && g.bias) {
-              q.x += g.bias[cbase + 4 * j];
-              q.y += g.bias[cbase + 4 * j + 1];
-              q.z += g.bias[cbase + 4 * j + 2];
-              q.w += g.bias[cbase + 4 * j + 3];
-            }
-            if (EPI == SS_EPI_F32_ADD)
-              atomicAdd(dst + j, q);
+            if (col + j >= g.N) break;
+            if (EPI == SS_EPI_BIAS_LRELU_BF16)
+              static_cast<bf16*>(g.c)[off + j] = __float2bfloat16_rn(x[j]);
+            else if (EPI == SS_EPI_F32_ADD)
+              atomicAdd(static_cast<float*>(g.c) + off + j, x[j]);
             else
-              dst[j] = q;
+              static_cast<float*>(g.c)[off + j] = x[j];
           }
         }
-        continue;
       }
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int col = n0 + c + j;
-        if (col >= g.N) break;
-        float x = v[j];
-        if (EPI == SS_EPI_F32) {
-          static_cast<float*>(g.c)[off + col] = x;
-        } else if (EPI == SS_EPI_F32_ADD) {
-          atomicAdd(static_cast<float*>(g.c) + off + col, x);
-        } else if (EPI == SS_EPI_BIAS_LRELU_BF16) {
-          x += g.bias ? g.bias[col] : 0.f;
-          x = x > 0.f ? x : g.slope * x;
-          static_cast<bf16*>(g.c)[off + col] = __float2bfloat16_rn(x);
-        } else {   // SS_EPI_BIAS_F32
-          static_cast<float*>(g.c)[off + col] = x + (g.bias ? g.bias[col] : 0.f);
-        }
-      }
+      __syncwarp();
     }
   }
   tc_fence_before();
@@ -214,7 +223,8 @@ int make_tmap(CUtensorMap* map, const void* ptr, long long k, long long rows, lo
 template <int BN, int EPI>
 int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits, cudaStream_t st) {
   auto kern = gemm_bf16_kernel<BN, EPI>;
-  constexpr size_t smem = gemm_smem_bytes<BN>();
+  constexpr size_t smem = gemm_smem_bytes<BN>();   // the attribute allows the full ring
+  const size_t smem_run = gemm_smem_bytes<BN>(g.stages);
   // the attribute is per device: set once on each device that launches this instantiation
   static std::mutex mu;
   static bool done[64] = {};
@@ -229,7 +239,7 @@ int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& 
     }
   }
   dim3 grid((g.N + BN - 1) / BN, (g.M + kBM - 1) / kBM, splits);
-  kern<<<grid, kGemmThreads, smem, st>>>(ta, tb, g);
+  kern<<<grid, kGemmThreads, smem_run, st>>>(ta, tb, g);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }
@@ -928,7 +938,7 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
   if (rc) return rc;
   rc = make_tmap(&tb, B, K, N, ldb, bn);
   if (rc) return rc;
-  GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err};
+  GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, std::min(kStagesG, per)};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   switch (bn) {
     case 32: return launch_gemm_bn<32>(epi, ta, tb, g, splits, st);

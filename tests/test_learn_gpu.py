@@ -30,7 +30,8 @@ def gemm(A, B, epi, bias=None, slope=0.2, out=None, splits=0):
 
 
 @pytest.mark.parametrize('M,N,K', [(200, 40, 40), (1000, 256, 1152), (300, 96, 520), (129, 300, 64),
-                                   (8192, 256, 2304), (64, 32, 9216)])
+                                   (8192, 256, 2304), (64, 32, 9216), (333, 37, 32), (40000, 576, 32),
+                                   (517, 130, 96)])
 def test_gemm_f32_matches_float32_matmul(M, N, K):
     from shotsweep_b200 import _lib
     g = torch.Generator(device='cuda').manual_seed(M * 7 + N + K)
@@ -56,12 +57,13 @@ def test_gemm_split_k_accumulates():
     assert err <= 1e-4 * ref.abs().max().item()
 
 
-def test_gemm_bias_leaky_relu_bf16():
+@pytest.mark.parametrize('N', [64, 37])
+def test_gemm_bias_leaky_relu_bf16(N):
     from shotsweep_b200 import _lib
     g = torch.Generator(device='cuda').manual_seed(5)
     A = torch.randn(517, 72, device='cuda', generator=g).to(torch.bfloat16)
-    B = torch.randn(64, 72, device='cuda', generator=g).to(torch.bfloat16)
-    bias = torch.randn(64, device='cuda', generator=g)
+    B = torch.randn(N, 72, device='cuda', generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device='cuda', generator=g)
     x = A.float() @ B.float().T + bias
     ref = torch.where(x > 0, x, 0.2 * x)
     got = gemm(A, B, _lib.EPI_BIAS_LRELU_BF16, bias=bias).float()
