@@ -404,6 +404,16 @@ typedef enum ss_gemm_epilogue {
 int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N, int32_t K,
                      int32_t epi, void* C, int64_t ldc, const float* bias, float slope, int32_t splits,
                      int32_t* err, void* stream);
+/* ss_gemm_bf16 with operands stored either way: `layout` bit 0 set means A is
+ * stored K-outer (A[k][m] at A + k*lda + m, lda >= M), bit 1 the same for B
+ * (B[k][n] at B + k*ldb + n, ldb >= N).  The tensor cores read such operands
+ * in place through M/N-major shared-memory descriptors, so C = A^T B^T-style
+ * products (a weight gradient from the activations as they are stored) need
+ * no transpose pass.  Layouts 0, 2 and 3; M/N-major strides obey the same
+ * multiple-of-8 and alignment rules. */
+int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N,
+                            int32_t K, int32_t layout, int32_t epi, void* C, int64_t ldc, const float* bias,
+                            float slope, int32_t splits, int32_t* err, void* stream);
 
 /* Convolution plumbing (NHWC BF16 activations).  conv[11] = {B, Hin, Win, Cin,
  * KH, KW, stride_h, stride_w, pad_h, pad_w, up}: the input is read through a
@@ -414,6 +424,9 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
  *   ss_col2im_lrelu_bf16  dpre[pixel][c] (row stride ldp) = leaky_relu'(y) x the
  *                         sum of the column gradients dcols [pixels_out][Kc]
  *                         that read input element (pixel, c); y: the input map
+ *   ss_col2im16_lrelu_bf16 the same with BF16 column gradients (Cin % 8 == 0,
+ *                         Kc % 8 == 0, 16-byte aligned dcols and y; at most
+ *                         2^31 - 1 input elements / 8)
  *   ss_im2col_both_bf16   cols [pixels][Kc] and, in the same pass, the columns
  *                         transposed [Kc][ldt] (Cin % 8 == 0, Kc == K): the
  *                         forward GEMM's operand and the weight gradient's
@@ -439,6 +452,8 @@ int32_t ss_im2col_both_bf16(const void* x, const int32_t* conv, int32_t Kc, void
                             void* stream);
 int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
                              void* dpre, int64_t ldp, void* stream);
+int32_t ss_col2im16_lrelu_bf16(const void* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
+                               void* dpre, int64_t ldp, void* stream);
 int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream);
 int32_t ss_transpose_sum_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out,
                               float* colsum, void* stream);

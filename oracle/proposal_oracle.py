@@ -3,8 +3,9 @@
 The network of shotsweep_b200/proposal.py (layer table LAYERS, flat parameter
 layout) as ordinary PyTorch operations on the CPU, differentiated by autograd.
 It rounds to BF16 exactly where the CUDA path stores BF16: the weights' BF16
-copy, every activation after its leaky ReLU, and every pre-activation gradient;
-everything else is float32.  Used only by tests/ to check the GPU forward pass
+copy, every activation after its leaky ReLU, every pre-activation gradient and
+every column gradient (the input-gradient GEMM's output, before col2im sums it
+onto the input); everything else is float32.  Used only by tests/ to check the GPU forward pass
 and every parameter gradient; nothing in the product imports it.
 """
 from __future__ import annotations
@@ -43,23 +44,12 @@ def loss_and_grads(params, x0, target):
     lay, total = param_layout()
     P = torch.tensor(np.asarray(params, np.float32), requires_grad=True)
     x = torch.as_tensor(x0, dtype=torch.float32)
-    B = x.shape[0]
-    for L, (hi, wi, ho, wo, K, Kc, N) in zip(LAYERS, plan_shapes()):
+    for L, shape in zip(LAYERS, plan_shapes()):
+        K, Kc, N = shape[4:]
         o, n = lay[L.name + '.w']
         W = RoundBF16.apply(P[o:o + n].view(N, Kc)[:, :K])
         ob, nb = lay[L.name + '.b']
-        b = P[ob:ob + nb]
-        if L.kind == 'conv':
-            xin = x.permute(0, 3, 1, 2)
-            if L.up > 1:
-                xin = F.interpolate(xin, scale_factor=L.up, mode='nearest')
-            w4 = W.reshape(N, L.kh, L.kw, L.cin).permute(0, 3, 1, 2)
-            pre = F.conv2d(xin, w4, b, stride=(L.sh, L.sw), padding=(L.ph, L.pw)).permute(0, 2, 3, 1)
-        elif L.kind == 'window':
-            pre = F.linear(x.reshape(B, -1), W, b).view(B, 1, 1, N)
-        else:
-            pre = F.linear(x.reshape(B, -1), W, b).view(B, L.out_hw, L.out_hw, L.cout)
-        pre = GradRoundBF16.apply(pre)
+        pre = GradRoundBF16.apply(_pre(L, shape, W, P[ob:ob + nb], x))
         x = RoundBF16.apply(F.leaky_relu(pre, SLOPE))
     o, n = lay['head.w']
     wh = P[o:o + n].view(3, 3, HEAD_C).permute(2, 0, 1)[None]
@@ -82,17 +72,20 @@ def adamw_step(p, g, m, v, step, lr, wd=1e-4, b1=0.9, b2=0.999, eps=1e-8):
 
 
 def _pre(L, shape, W, b, x):
+    """Pre-activation [B, ho, wo, N] as columns x weights^T + bias; the columns' gradient is rounded to BF16."""
     hi, wi, ho, wo, K, Kc, N = shape
     B = x.shape[0]
     if L.kind == 'conv':
         xin = x.permute(0, 3, 1, 2)
         if L.up > 1:
             xin = F.interpolate(xin, scale_factor=L.up, mode='nearest')
-        w4 = W.reshape(N, L.kh, L.kw, L.cin).permute(0, 3, 1, 2)
-        return F.conv2d(xin, w4, b, stride=(L.sh, L.sw), padding=(L.ph, L.pw)).permute(0, 2, 3, 1)
+        u = F.unfold(xin, (L.kh, L.kw), padding=(L.ph, L.pw), stride=(L.sh, L.sw))     # [B, (c, kh, kw), pixels]
+        cols = u.view(B, L.cin, L.kh * L.kw, -1).permute(0, 3, 2, 1).reshape(B, -1, K)  # [B, pixels, (kh, kw, c)]
+        return F.linear(GradRoundBF16.apply(cols), W, b).view(B, ho, wo, N)
+    cols = GradRoundBF16.apply(x.reshape(B, -1))
     if L.kind == 'window':
-        return F.linear(x.reshape(B, -1), W, b).view(B, 1, 1, N)
-    return F.linear(x.reshape(B, -1), W, b).view(B, L.out_hw, L.out_hw, L.cout)
+        return F.linear(cols, W, b).view(B, 1, 1, N)
+    return F.linear(cols, W, b).view(B, L.out_hw, L.out_hw, L.cout)
 
 
 def layer_weights(params, i):

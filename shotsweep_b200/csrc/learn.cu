@@ -53,7 +53,9 @@ constexpr size_t gemm_smem_bytes(int stages = kStagesG) {
   return 1024 + static_cast<size_t>(stages) * (kBM * 128 + BN * 128) + (2 * kStagesG + 1) * 8 + 16;
 }
 
-template <int BN, int EPI>
+// AMN / BMN: operand stored K-outer (A[k][m], B[k][n]) and read in place
+// through MN-major descriptors, two (A) or BN/64 (B) 64 x 64 boxes per stage.
+template <int BN, int EPI, bool AMN, bool BMN>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const GemmArgs g) {
   using namespace sm100;
@@ -94,21 +96,35 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       const int s = i % ns;
       if (i >= ns && !mbar_wait(empty(s), ((i / ns) - 1) & 1, g.err, 1)) break;
       mbar_expect_tx(full(s), STAGE);
-      tma_load_2d(sbase + s * STAGE, &ta, (kt0 + i) * kBK, m0, full(s));
-      tma_load_2d(sbase + s * STAGE + A_BYTES, &tb, (kt0 + i) * kBK, n0, full(s));
+      const int kc = (kt0 + i) * kBK;
+      const uint32_t sa = sbase + s * STAGE, sb = sa + A_BYTES;
+      if (AMN) {
+#pragma unroll
+        for (int j = 0; j < kBM / 64; ++j) tma_load_2d(sa + j * 8192, &ta, m0 + 64 * j, kc, full(s));
+      } else {
+        tma_load_2d(sa, &ta, kc, m0, full(s));
+      }
+      if (BMN) {
+#pragma unroll
+        for (int j = 0; j < BN / 64; ++j) tma_load_2d(sb + j * 8192, &tb, n0 + 64 * j, kc, full(s));
+      } else {
+        tma_load_2d(sb, &tb, kc, n0, full(s));
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer: four K=16 MMAs per stage, the stage freed on completion
-    constexpr uint32_t idesc = idesc_bf16_f32(kBM, BN);
+    constexpr uint32_t idesc = idesc_bf16_f32(kBM, BN, AMN, BMN);
+    constexpr uint32_t a_step = AMN ? 2048 >> 4 : 32 >> 4, b_step = BMN ? 2048 >> 4 : 32 >> 4;   // per K=16
     for (int i = 0; i < nk; ++i) {
       const int s = i % ns;
       if (!mbar_wait(full(s), (i / ns) & 1, g.err, 2)) break;
       tc_fence_after();
-      const uint64_t da = desc_sw128_kmajor(sbase + s * STAGE);
-      const uint64_t db = desc_sw128_kmajor(sbase + s * STAGE + A_BYTES);
+      const uint32_t sa = sbase + s * STAGE, sb = sa + A_BYTES;
+      const uint64_t da = AMN ? desc_sw128_mnmajor(sa, 8192) : desc_sw128_kmajor(sa);
+      const uint64_t db = BMN ? desc_sw128_mnmajor(sb, 8192) : desc_sw128_kmajor(sb);
 #pragma unroll
       for (int kk = 0; kk < kBK / 16; ++kk)
-        mma_bf16(taddr, da + 2 * kk, db + 2 * kk, idesc, (i > 0 || kk > 0) ? 1u : 0u);
+        mma_bf16(taddr, da + a_step * kk, db + b_step * kk, idesc, (i > 0 || kk > 0) ? 1u : 0u);
       mma_commit(empty(s));
     }
     mma_commit(acc_bar);
@@ -220,9 +236,9 @@ int make_tmap(CUtensorMap* map, const void* ptr, long long k, long long rows, lo
   return SS_OK;
 }
 
-template <int BN, int EPI>
+template <int BN, int EPI, bool AMN, bool BMN>
 int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits, cudaStream_t st) {
-  auto kern = gemm_bf16_kernel<BN, EPI>;
+  auto kern = gemm_bf16_kernel<BN, EPI, AMN, BMN>;
   constexpr size_t smem = gemm_smem_bytes<BN>();   // the attribute allows the full ring
   const size_t smem_run = gemm_smem_bytes<BN>(g.stages);
   // the attribute is per device: set once on each device that launches this instantiation
@@ -244,15 +260,27 @@ int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& 
   return SS_OK;
 }
 
-template <int BN>
-int launch_gemm_bn(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits,
-                   cudaStream_t st) {
+template <int BN, bool AMN, bool BMN>
+int launch_gemm_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits,
+                    cudaStream_t st) {
   switch (epi) {
-    case SS_EPI_F32: return launch_gemm_t<BN, SS_EPI_F32>(ta, tb, g, splits, st);
-    case SS_EPI_F32_ADD: return launch_gemm_t<BN, SS_EPI_F32_ADD>(ta, tb, g, splits, st);
-    case SS_EPI_BIAS_LRELU_BF16: return launch_gemm_t<BN, SS_EPI_BIAS_LRELU_BF16>(ta, tb, g, splits, st);
-    default: return launch_gemm_t<BN, SS_EPI_BIAS_F32>(ta, tb, g, splits, st);
+    case SS_EPI_F32: return launch_gemm_t<BN, SS_EPI_F32, AMN, BMN>(ta, tb, g, splits, st);
+    case SS_EPI_F32_ADD: return launch_gemm_t<BN, SS_EPI_F32_ADD, AMN, BMN>(ta, tb, g, splits, st);
+    case SS_EPI_BIAS_LRELU_BF16: return launch_gemm_t<BN, SS_EPI_BIAS_LRELU_BF16, AMN, BMN>(ta, tb, g, splits, st);
+    default: return launch_gemm_t<BN, SS_EPI_BIAS_F32, AMN, BMN>(ta, tb, g, splits, st);
   }
+}
+
+// layout bit 0: A stored K-outer; bit 1: B stored K-outer (layouts 0, 2 and 3).
+// An MN-major B needs whole 64-column boxes, so its tiles are at least 64 wide.
+template <int BN>
+int launch_gemm_bn(int layout, int epi, const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits,
+                   cudaStream_t st) {
+  if constexpr (BN >= 64) {
+    if (layout == 3) return launch_gemm_epi<BN, true, true>(epi, ta, tb, g, splits, st);
+    if (layout == 2) return launch_gemm_epi<BN, false, true>(epi, ta, tb, g, splits, st);
+  }
+  return launch_gemm_epi<BN, false, false>(epi, ta, tb, g, splits, st);
 }
 
 
@@ -458,6 +486,61 @@ __global__ void col2im_lrelu_vec4_kernel(const float* __restrict__ dcols, ConvGe
   }
 }
 
+// BF16 column gradients back onto the input, 8 channels per thread (16-byte
+// loads and stores), times the leaky-ReLU derivative of the layer below.
+// Indices are 32-bit (the host checks the element count): the per-thread
+// divisions are what bounds a gather this short.
+__global__ void __launch_bounds__(256) col2im16_lrelu_kernel(const bf16* __restrict__ dcols, ConvGeom g, int Kc,
+                                                             const bf16* __restrict__ y, float slope,
+                                                             bf16* __restrict__ dpre, int64_t ldp, int total) {
+  const int c8n = g.Cin >> 3;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const int pix = i / c8n;
+    const int c = (i - pix * c8n) * 8;
+    const int ix = pix % g.Win, t = pix / g.Win;
+    const int iy = t % g.Hin, b = t / g.Hin;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int uy = iy * g.up; uy < (iy + 1) * g.up; ++uy)
+      for (int kh = 0; kh < g.KH; ++kh) {
+        const int ty = uy + g.ph - kh;
+        if (ty < 0 || ty % g.sh) continue;
+        const int oy = ty / g.sh;
+        if (oy >= g.Hout) continue;
+        const bf16* rowp = dcols + (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout * Kc + kh * g.KW * g.Cin + c;
+        for (int ux = ix * g.up; ux < (ix + 1) * g.up; ++ux)
+          for (int kw = 0; kw < g.KW; ++kw) {
+            const int tx = ux + g.pw - kw;
+            if (tx < 0 || tx % g.sw) continue;
+            const int ox = tx / g.sw;
+            if (ox >= g.Wout) continue;
+            const uint4 d = *reinterpret_cast<const uint4*>(rowp + static_cast<int64_t>(ox) * Kc + kw * g.Cin);
+            const uint32_t w[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              acc[2 * j] += __uint_as_float(w[j] << 16);
+              acc[2 * j + 1] += __uint_as_float(w[j] & 0xffff0000u);
+            }
+          }
+      }
+    const uint4 yv = *reinterpret_cast<const uint4*>(y + static_cast<int64_t>(pix) * g.Cin + c);
+    const uint32_t yw[4] = {yv.x, yv.y, yv.z, yv.w};
+    __align__(16) bf16 o[8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float y0 = __uint_as_float(yw[j] << 16), y1 = __uint_as_float(yw[j] & 0xffff0000u);
+      o[2 * j] = __float2bfloat16_rn(y0 > 0.f ? acc[2 * j] : slope * acc[2 * j]);
+      o[2 * j + 1] = __float2bfloat16_rn(y1 > 0.f ? acc[2 * j + 1] : slope * acc[2 * j + 1]);
+    }
+    bf16* dst = dpre + static_cast<int64_t>(pix) * ldp + c;
+    if ((ldp & 7) == 0 && (reinterpret_cast<uintptr_t>(dpre) & 15) == 0) {
+      *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(o);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) dst[j] = o[j];
+    }
+  }
+}
+
 // Column gradients back onto the input (the transpose of im2col, as a
 // gather: no atomics, deterministic), times the leaky-ReLU derivative of the
 // layer below, whose output y is the input here: dpre = dx * (y > 0 ? 1 : slope).
@@ -591,6 +674,50 @@ __global__ void bias_grad_kernel(const bf16* __restrict__ dpre, int64_t ld, int6
   float acc = 0.f;
   for (int64_t m = blockIdx.y; m < M; m += gridDim.y) acc += __bfloat162float(dpre[m * ld + c]);
   atomicAdd(db + c, acc);
+}
+
+// Column sums with 16-byte loads (C % 8 == 0, ld % 8 == 0, aligned base): a
+// CTA sums a slab of rows; L threads span a row's column groups of 8, R = 256
+// / L rows are read at once, and the R partial sums of a column group meet in
+// shared memory before one atomic per column and CTA.
+__global__ void __launch_bounds__(256) bias_grad_v8_kernel(const bf16* __restrict__ dpre, int64_t ld, int64_t M,
+                                                           int C, int64_t rows_per_cta, float* __restrict__ db) {
+  __shared__ float red[256 * 8];
+  const int G = C >> 3, L = G < 256 ? G : 256, R = 256 / L;
+  const int t = threadIdx.x, cgi = t % L, rr = t / L;
+  const int64_t r0 = blockIdx.x * rows_per_cta;
+  const int64_t r1 = r0 + rows_per_cta < M ? r0 + rows_per_cta : M;
+  for (int cg0 = 0; cg0 < G; cg0 += L) {
+    const int cg = cg0 + cgi;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (rr < R && cg < G) {
+      for (int64_t r = r0 + rr; r < r1; r += R) {
+        const uint4 v = *reinterpret_cast<const uint4*>(dpre + r * ld + cg * 8);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[2 * j] += __uint_as_float(w[j] << 16);
+          acc[2 * j + 1] += __uint_as_float(w[j] & 0xffff0000u);
+        }
+      }
+    }
+    if (R > 1) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) red[t * 8 + j] = acc[j];
+      __syncthreads();
+      if (rr == 0 && cg < G) {
+        for (int q = 1; q < R; ++q)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[j] += red[(q * L + cgi) * 8 + j];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) atomicAdd(db + cg * 8 + j, acc[j]);
+      }
+      __syncthreads();
+    } else if (cg < G) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) atomicAdd(db + cg * 8 + j, acc[j]);
+    }
+  }
 }
 
 // Output head: crop rows/cols [off, off+n) of x [B][H][W][C], 3x3 convolution
@@ -911,16 +1038,18 @@ ConvGeom conv_geom(const int32_t* d) {
 
 extern "C" {
 
-int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N, int32_t K,
-                     int32_t epi, void* C, int64_t ldc, const float* bias, float slope, int32_t splits, int32_t* err,
-                     void* stream) {
+int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N,
+                            int32_t K, int32_t layout, int32_t epi, void* C, int64_t ldc, const float* bias,
+                            float slope, int32_t splits, int32_t* err, void* stream) {
   ss_internal::clear_error();
-  if (!A || !B || !C || !err || M < 1 || N < 1 || K < 1 || lda < K || ldb < K || ldc < N)
+  if (layout != 0 && layout != 2 && layout != 3) return fail(SS_ERR_INVALID, "GEMM operand layout must be 0, 2 or 3");
+  const bool amn = layout & 1, bmn = layout & 2;
+  if (!A || !B || !C || !err || M < 1 || N < 1 || K < 1 || lda < (amn ? M : K) || ldb < (bmn ? N : K) || ldc < N)
     return fail(SS_ERR_INVALID, "bad GEMM arguments");
   if (epi < SS_EPI_F32 || epi > SS_EPI_BIAS_F32) return fail(SS_ERR_INVALID, "unknown GEMM epilogue");
   const int k_tiles = (K + kBK - 1) / kBK;
   // tile width: the smallest of 32 / 64 / 128 covering N, 256 for wide outputs with enough row tiles
-  int bn = N <= 32 ? 32 : N <= 64 ? 64 : 128;
+  int bn = N <= 32 && !bmn ? 32 : N <= 64 ? 64 : 128;
   const int m_tiles = (M + kBM - 1) / kBM;
   if (N >= 256 && m_tiles * ((N + 255) / 256) >= 148) bn = 256;
   const int tiles = m_tiles * ((N + bn - 1) / bn);
@@ -933,19 +1062,26 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
   splits = std::min(splits, k_tiles);
   const int per = (k_tiles + splits - 1) / splits;
   splits = (k_tiles + per - 1) / per;   // every split gets at least one K tile
+  // K-major operands: boxes of 64 K x the tile's rows; MN-major: boxes of 64 x 64 (M/N innermost)
   CUtensorMap ta, tb;
-  int rc = make_tmap(&ta, A, K, M, lda, kBM);
+  int rc = amn ? make_tmap(&ta, A, M, K, lda, 64) : make_tmap(&ta, A, K, M, lda, kBM);
   if (rc) return rc;
-  rc = make_tmap(&tb, B, K, N, ldb, bn);
+  rc = bmn ? make_tmap(&tb, B, N, K, ldb, 64) : make_tmap(&tb, B, K, N, ldb, bn);
   if (rc) return rc;
   GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, std::min(kStagesG, per)};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   switch (bn) {
-    case 32: return launch_gemm_bn<32>(epi, ta, tb, g, splits, st);
-    case 64: return launch_gemm_bn<64>(epi, ta, tb, g, splits, st);
-    case 128: return launch_gemm_bn<128>(epi, ta, tb, g, splits, st);
-    default: return launch_gemm_bn<256>(epi, ta, tb, g, splits, st);
+    case 32: return launch_gemm_bn<32>(layout, epi, ta, tb, g, splits, st);
+    case 64: return launch_gemm_bn<64>(layout, epi, ta, tb, g, splits, st);
+    case 128: return launch_gemm_bn<128>(layout, epi, ta, tb, g, splits, st);
+    default: return launch_gemm_bn<256>(layout, epi, ta, tb, g, splits, st);
   }
+}
+
+int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int32_t M, int32_t N, int32_t K,
+                     int32_t epi, void* C, int64_t ldc, const float* bias, float slope, int32_t splits, int32_t* err,
+                     void* stream) {
+  return ss_gemm_bf16_layout(A, lda, B, ldb, M, N, K, 0, epi, C, ldc, bias, slope, splits, err, stream);
 }
 
 // conv: {B, Hin, Win, Cin, KH, KW, sh, sw, ph, pw, up}; the output size follows.
@@ -1013,6 +1149,26 @@ int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc
   return SS_OK;
 }
 
+int32_t ss_col2im16_lrelu_bf16(const void* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
+                               void* dpre, int64_t ldp, void* stream) {
+  ss_internal::clear_error();
+  if (!dcols || !conv || !y || !dpre) return fail(SS_ERR_INVALID, "bad arguments");
+  const ConvGeom g = conv_geom(conv);
+  if (g.B < 1 || g.Hin < 1 || g.Win < 1 || g.Cin < 1 || g.Hout < 1 || g.Wout < 1 || g.sh < 1 || g.sw < 1 || g.up < 1)
+    return fail(SS_ERR_INVALID, "bad convolution geometry");
+  if (ldp < g.Cin) return fail(SS_ERR_INVALID, "ldp < channels");
+  if (g.Cin % 8 || Kc % 8 || Kc < g.KH * g.KW * g.Cin || (reinterpret_cast<uintptr_t>(dcols) & 15) ||
+      (reinterpret_cast<uintptr_t>(y) & 15))
+    return fail(SS_ERR_UNSUPPORTED, "BF16 column gradients need Cin % 8 == 0, Kc % 8 == 0 and 16-byte aligned buffers");
+  const long long total = static_cast<long long>(g.B) * g.Hin * g.Win * (g.Cin / 8);
+  if (total >= (1LL << 31)) return fail(SS_ERR_UNSUPPORTED, "too many input elements for one launch");
+  col2im16_lrelu_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const bf16*>(dcols), g, Kc, static_cast<const bf16*>(y), slope, static_cast<bf16*>(dpre), ldp,
+      static_cast<int>(total));
+  SS_TRY_CUDA(cudaGetLastError());
+  return SS_OK;
+}
+
 // Transpose (and optionally column sums) through the pair-wise kernel when
 // strides and addresses allow 4-byte BF16-pair accesses, else element-wise.
 static int transpose_launch(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, float* colsum,
@@ -1064,8 +1220,16 @@ int32_t ss_transpose_sum_bf16(const void* in, int64_t ld_in, int32_t R, int32_t 
 int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream) {
   ss_internal::clear_error();
   if (!dpre || !db || M < 1 || C < 1 || ld < C) return fail(SS_ERR_INVALID, "bad arguments");
-  dim3 grid((C + 127) / 128, static_cast<unsigned>(std::min<long long>(M, 512)));
-  bias_grad_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(dpre), ld, M, C, db);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (C % 8 == 0 && ld % 8 == 0 && (reinterpret_cast<uintptr_t>(dpre) & 15) == 0) {
+    const long long ctas = std::max(1LL, std::min((static_cast<long long>(M) + 255) / 256, 148LL * 8));
+    const long long rows = (M + ctas - 1) / ctas;
+    bias_grad_v8_kernel<<<static_cast<unsigned>((M + rows - 1) / rows), 256, 0, st>>>(static_cast<const bf16*>(dpre),
+                                                                                      ld, M, C, rows, db);
+  } else {
+    dim3 grid((C + 127) / 128, static_cast<unsigned>(std::min<long long>(M, 512)));
+    bias_grad_kernel<<<grid, 128, 0, st>>>(static_cast<const bf16*>(dpre), ld, M, C, db);
+  }
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }

@@ -129,9 +129,24 @@ __device__ __forceinline__ uint64_t desc_sw128_kmajor(uint32_t smem_addr) {
   d |= static_cast<uint64_t>(2u) << 61;                             // 128-byte swizzle
   return d;
 }
-// Instruction descriptor: BF16 x BF16 -> F32, both operands K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+// Shared-memory descriptor of an MN-major tile written by TMA with 128-byte
+// swizzling: boxes of 64 K rows x 64 M/N elements (8 KB), `atom_stride` bytes
+// apart along M/N (the leading byte offset); 8-row groups along K are 1024 B
+// apart (the stride byte offset).  A K=16 slice starts 16 rows (2048 B) on.
+__device__ __forceinline__ uint64_t desc_sw128_mnmajor(uint32_t smem_addr, uint32_t atom_stride) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu);          // start address
+  d |= static_cast<uint64_t>((atom_stride >> 4) & 0x3FFFu) << 16;   // leading byte offset: next 64 along M/N
+  d |= static_cast<uint64_t>(1024u >> 4) << 32;                     // stride byte offset: next 8 rows along K
+  d |= static_cast<uint64_t>(1u) << 46;                             // descriptor version (sm_100)
+  d |= static_cast<uint64_t>(2u) << 61;                             // 128-byte swizzle
+  return d;
+}
+// Instruction descriptor: BF16 x BF16 -> F32, M x N; a_mn / b_mn mark an
+// operand stored M/N-major (transposed) in shared memory.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N, bool a_mn = false, bool b_mn = false) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(a_mn) << 15) |
+         (static_cast<uint32_t>(b_mn) << 16) | (static_cast<uint32_t>(N >> 3) << 17) |
          (static_cast<uint32_t>(M >> 4) << 24);
 }
 

@@ -153,23 +153,13 @@ class ProposalNet:
         self.x0 = torch.empty(B * T_IN * X_IN * S_IN, **bf)
         self.y = []
         self.cols = []       # each convolution's im2col columns, kept from forward to backward
-        self.colst_l = []    # and their transpose, written in the same pass where the channels allow
-        max_colst = max_dcols = max_wt = max_dpret = 1
+        max_dcols = 1
         for L, (hi, wi, ho, wo, K, Kc, N) in zip(LAYERS, self.shapes):
             M = B * (ho * wo if L.kind != 'fc' else 1)
             self.y.append(torch.empty(M * N, **bf))
             self.cols.append(torch.empty(M * Kc, **bf) if L.kind == 'conv' else None)
-            both = L.kind == 'conv' and L.cin % 8 == 0 and K == Kc
-            self.colst_l.append(torch.empty(K * round8(M), **bf) if both else None)
-            if not both:
-                max_colst = max(max_colst, K * round8(M))
             max_dcols = max(max_dcols, M * K)
-            max_wt = max(max_wt, K * round8(N))
-            max_dpret = max(max_dpret, N * round8(M))
-        self.colst = torch.empty(max_colst, **bf)
-        self.dcols = torch.empty(max_dcols, **f32)
-        self.wt = torch.empty(max_wt, **bf)
-        self.dpret = torch.empty(max_dpret, **bf)
+        self.dcols = torch.empty(max_dcols, **bf)   # column gradients, BF16 (rounded once, summed in F32 by col2im)
         self.dpre = [torch.empty_like(y) for y in self.y]
         self.pred = torch.empty(B, OUT, OUT, **f32)
         self.target = torch.empty(B, OUT, OUT, **f32)
@@ -206,9 +196,11 @@ class ProposalNet:
     def _stream(self):
         return _lib.stream_handle(self.dev)
 
-    def _gemm(self, A, lda, Bm, ldb, M, N, K, epi, C, ldc, bias=None):
-        _lib.check(self.L.ss_gemm_bf16(_lib.ptr(A), lda, _lib.ptr(Bm), ldb, M, N, K, epi, _lib.ptr(C), ldc,
-                                       _lib.ptr(bias), SLOPE, 0, _lib.ptr(self.err), self._stream()), 'ss_gemm_bf16')
+    def _gemm(self, A, lda, Bm, ldb, M, N, K, epi, C, ldc, bias=None, slope=SLOPE, layout=0):
+        """C = A B^T through the tensor cores; layout bit 0 / 1: A / B stored K-outer (read M/N-major)."""
+        _lib.check(self.L.ss_gemm_bf16_layout(_lib.ptr(A), lda, _lib.ptr(Bm), ldb, M, N, K, layout, epi, _lib.ptr(C),
+                                              ldc, _lib.ptr(bias), slope, 0, _lib.ptr(self.err), self._stream()),
+                   'ss_gemm_bf16_layout')
 
     # -- forward / backward -------------------------------------------------------
     def load_batch(self, stored, scale, targets=None):
@@ -225,13 +217,8 @@ class ProposalNet:
             hi, wi, ho, wo, K, Kc, N = self.shapes[i]
             M = self.B * (ho * wo if L.kind != 'fc' else 1)
             if L.kind == 'conv':
-                if self.colst_l[i] is not None:   # the columns and their transpose for the weight gradient
-                    _lib.check(self.L.ss_im2col_both_bf16(_lib.ptr(x), self._conv(i), Kc, _lib.ptr(self.cols[i]),
-                                                          _lib.ptr(self.colst_l[i]), round8(M), self._stream()),
-                               'ss_im2col_both_bf16')
-                else:
-                    _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols[i]),
-                                                     self._stream()), 'ss_im2col_bf16')
+                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols[i]),
+                                                 self._stream()), 'ss_im2col_bf16')
                 A, lda = self.cols[i], Kc
             else:
                 A, lda = x, K
@@ -261,29 +248,23 @@ class ProposalNet:
             M = self.B * (ho * wo if L.kind != 'fc' else 1)
             x = self.x0 if i == 0 else self.y[i - 1]
             dp = self.dpre[i]
-            M8 = round8(M)
-            # the transposed pre-activation gradient for the weight gradient, and the bias gradient, in one pass
-            _lib.check(self.L.ss_transpose_sum_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self.dpret), M8,
-                                                    _lib.ptr(self._view(self.grads, L.name + '.b')), self._stream()),
-                       'ss_transpose_sum_bf16')
-            colst = self.colst_l[i]
-            if colst is None:
-                src, lds = (self.cols[i], Kc) if L.kind == 'conv' else (x, K)   # forward columns, or the input itself
-                _lib.check(self.L.ss_transpose_bf16(_lib.ptr(src), lds, M, K, _lib.ptr(self.colst), M8, self._stream()),
-                           'ss_transpose_bf16')
-                colst = self.colst
-            self._gemm(self.dpret, M8, colst, M8, N, K, M, _lib.EPI_F32_ADD,
-                       self._view(self.grads, L.name + '.w'), Kc)
+            # bias gradient: column sums of the pre-activation gradient
+            _lib.check(self.L.ss_bias_grad_bf16(_lib.ptr(dp), N, M, N, _lib.ptr(self._view(self.grads, L.name + '.b')),
+                                                self._stream()), 'ss_bias_grad_bf16')
+            # weight gradient dW[N][K] += dp^T cols: both operands read as stored (pixels outermost)
+            src, lds = (self.cols[i], Kc) if L.kind == 'conv' else (x, K)   # forward columns, or the input itself
+            self._gemm(dp, N, src, lds, N, K, M, _lib.EPI_F32_ADD, self._view(self.grads, L.name + '.w'), Kc,
+                       layout=3)
             if i == 0:
                 break
-            N8 = round8(N)
-            _lib.check(self.L.ss_transpose_bf16(_lib.ptr(self.weight16(i)), Kc, N, K, _lib.ptr(self.wt), N8,
-                                                self._stream()), 'ss_transpose_bf16')
-            self._gemm(dp, N, self.wt, N8, M, K, N, _lib.EPI_F32, self.dcols, K)
+            # column gradients dcols[M][K] = dp W (weights read as stored, [N][Kc]), rounded to BF16 (slope 1, no
+            # bias: a plain BF16 store), then gathered onto the input
+            self._gemm(dp, N, self.weight16(i), Kc, M, K, N, _lib.EPI_BIAS_LRELU_BF16, self.dcols, K, slope=1.0,
+                       layout=2)
             Lp = LAYERS[i - 1]
-            _lib.check(self.L.ss_col2im_lrelu_bf16(_lib.ptr(self.dcols), self._conv(i), K, _lib.ptr(x), SLOPE,
-                                                   _lib.ptr(self.dpre[i - 1]), Lp.cout, self._stream()),
-                       'ss_col2im_lrelu_bf16')
+            _lib.check(self.L.ss_col2im16_lrelu_bf16(_lib.ptr(self.dcols), self._conv(i), K, _lib.ptr(x), SLOPE,
+                                                     _lib.ptr(self.dpre[i - 1]), Lp.cout, self._stream()),
+                       'ss_col2im16_lrelu_bf16')
 
     def optimizer_step(self, weight_decay=1e-4):
         _lib.check(self.L.ss_adamw(_lib.ptr(self.params), _lib.ptr(self.grads), _lib.ptr(self.m), _lib.ptr(self.v),

@@ -45,6 +45,41 @@ def test_gemm_f32_matches_float32_matmul(M, N, K):
     assert torch.allclose(got, ref + bias, rtol=0, atol=GEMM_TOL * ref.abs().max().item() * 10 + 1e-6 * K ** 0.5)
 
 
+@pytest.mark.parametrize('M,N,K,layout,epi', [(32, 576, 4000, 3, 'add'), (64, 40, 1000, 3, 'add'),
+                                                (256, 128, 777, 3, 'add'), (136, 64, 96, 3, 'f32'),
+                                                (1000, 576, 32, 2, 'bf16'), (300, 136, 200, 2, 'f32'),
+                                                (4096, 1152, 128, 2, 'bf16')])
+def test_gemm_operand_layouts(M, N, K, layout, epi):
+    """Operands stored K-outer and read in place through M/N-major descriptors (the weight-gradient and
+    input-gradient GEMMs of the proposal network) give the K-major product: the same BF16 values multiplied in
+    float32, split-K accumulation and the BF16 epilogue included."""
+    from shotsweep_b200 import _lib
+    g = torch.Generator(device='cuda').manual_seed(M + 3 * N + 7 * K + layout)
+    A = torch.randn(M, K, device='cuda', generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device='cuda', generator=g).to(torch.bfloat16)
+    ref = A.float() @ B.float().T
+    As = A.T.contiguous() if layout & 1 else A
+    Bs = B.T.contiguous() if layout & 2 else B
+    code = {'add': _lib.EPI_F32_ADD, 'f32': _lib.EPI_F32, 'bf16': _lib.EPI_BIAS_LRELU_BF16}[epi]
+    start = torch.randn(M, N, device='cuda', generator=g) if epi == 'add' else None
+    out = start.clone() if epi == 'add' else torch.zeros(M, N, device='cuda', dtype=torch.bfloat16 if epi == 'bf16'
+                                                         else torch.float32)
+    err = torch.zeros(1, dtype=torch.int32, device='cuda')
+    L = _lib.load()
+    _lib.check(L.ss_gemm_bf16_layout(_lib.ptr(As), As.stride(0), _lib.ptr(Bs), Bs.stride(0), M, N, K, layout, code,
+                                     _lib.ptr(out), out.stride(0), None, 1.0, 0, _lib.ptr(err),
+                                     _lib.stream_handle(A.device)), 'ss_gemm_bf16_layout')
+    torch.cuda.synchronize()
+    assert err.item() == 0
+    if epi == 'add':
+        ref = ref + start
+    scale = ref.abs().max().item()
+    if epi == 'bf16':   # one BF16 rounding of the float32 product
+        assert ((out.float() - ref).abs() <= 2 ** -8 * ref.abs() + 1e-5 * scale).all()
+    else:
+        assert (out - ref).abs().max().item() <= 1e-5 * scale * 10 + 1e-6 * K ** 0.5
+
+
 def test_gemm_split_k_accumulates():
     from shotsweep_b200 import _lib
     g = torch.Generator(device='cuda').manual_seed(11)
