@@ -488,30 +488,40 @@ __global__ void col2im_lrelu_vec4_kernel(const float* __restrict__ dcols, ConvGe
 
 // BF16 column gradients back onto the input, 8 channels per thread (16-byte
 // loads and stores), times the leaky-ReLU derivative of the layer below.
-// Indices are 32-bit (the host checks the element count): the per-thread
-// divisions are what bounds a gather this short.
+// The tap geometry (KH, KW, strides, upsampling) is a template parameter for
+// the network's layer families (0: read at run time), so the stride tests and
+// divisions of the tap loops fold to constants; the per-thread index work
+// otherwise bounds a gather this short.  Indices are 32-bit (the host checks
+// the element count); Cin / 8 is a power of two (c8_shift).
+template <int KH_, int KW_, int SH_, int SW_, int UP_>
 __global__ void __launch_bounds__(256) col2im16_lrelu_kernel(const bf16* __restrict__ dcols, ConvGeom g, int Kc,
                                                              const bf16* __restrict__ y, float slope,
-                                                             bf16* __restrict__ dpre, int64_t ldp, int total) {
-  const int c8n = g.Cin >> 3;
+                                                             bf16* __restrict__ dpre, int64_t ldp, int total,
+                                                             int c8_shift) {
+  const int KH = KH_ ? KH_ : g.KH, KW = KW_ ? KW_ : g.KW, SH = SH_ ? SH_ : g.sh, SW = SW_ ? SW_ : g.sw;
+  const int UP = UP_ ? UP_ : g.up;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const int pix = i / c8n;
-    const int c = (i - pix * c8n) * 8;
+    const int pix = i >> c8_shift;
+    const int c = (i - (pix << c8_shift)) * 8;
     const int ix = pix % g.Win, t = pix / g.Win;
     const int iy = t % g.Hin, b = t / g.Hin;
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int uy = iy * g.up; uy < (iy + 1) * g.up; ++uy)
-      for (int kh = 0; kh < g.KH; ++kh) {
-        const int ty = uy + g.ph - kh;
-        if (ty < 0 || ty % g.sh) continue;
-        const int oy = ty / g.sh;
+#pragma unroll
+    for (int dy = 0; dy < UP; ++dy)
+#pragma unroll
+      for (int kh = 0; kh < KH; ++kh) {
+        const int ty = iy * UP + dy + g.ph - kh;
+        if (ty < 0 || ty % SH) continue;
+        const int oy = ty / SH;
         if (oy >= g.Hout) continue;
-        const bf16* rowp = dcols + (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout * Kc + kh * g.KW * g.Cin + c;
-        for (int ux = ix * g.up; ux < (ix + 1) * g.up; ++ux)
-          for (int kw = 0; kw < g.KW; ++kw) {
-            const int tx = ux + g.pw - kw;
-            if (tx < 0 || tx % g.sw) continue;
-            const int ox = tx / g.sw;
+        const bf16* rowp = dcols + (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout * Kc + kh * KW * g.Cin + c;
+#pragma unroll
+        for (int dx = 0; dx < UP; ++dx)
+#pragma unroll
+          for (int kw = 0; kw < KW; ++kw) {
+            const int tx = ix * UP + dx + g.pw - kw;
+            if (tx < 0 || tx % SW) continue;
+            const int ox = tx / SW;
             if (ox >= g.Wout) continue;
             const uint4 d = *reinterpret_cast<const uint4*>(rowp + static_cast<int64_t>(ox) * Kc + kw * g.Cin);
             const uint32_t w[4] = {d.x, d.y, d.z, d.w};
@@ -537,6 +547,38 @@ __global__ void __launch_bounds__(256) col2im16_lrelu_kernel(const bf16* __restr
     } else {
 #pragma unroll
       for (int j = 0; j < 8; ++j) dst[j] = o[j];
+    }
+  }
+}
+
+// im2col in 16-byte chunks (Cin % 8 == 0, Kc == K, Cin / 8 a power of two):
+// 2^lanes_shift consecutive threads share one output pixel, whose coordinates
+// they work out once, and write its column row chunk by chunk (a warp's
+// stores cover whole rows); a chunk costs a shift, the tap split (a constant
+// KW) and one 16-byte load and store.  32-bit indices (checked on the host).
+template <int KW_, int UP_>
+__global__ void __launch_bounds__(256) im2col_px_kernel(const bf16* __restrict__ x, ConvGeom g, int M, int chunks,
+                                                        int c8_shift, int lanes_shift, bf16* __restrict__ cols) {
+  const int KW = KW_ ? KW_ : g.KW, UP = UP_ ? UP_ : g.up;
+  const int lanes = 1 << lanes_shift;
+  const int sub = threadIdx.x & (lanes - 1);
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> lanes_shift;
+  const int ngroups = (gridDim.x * blockDim.x) >> lanes_shift;
+  const int Hup = g.Hin * UP, Wup = g.Win * UP;
+  for (int m = group; m < M; m += ngroups) {
+    const int ox = m % g.Wout, t = m / g.Wout;
+    const int oy = t % g.Hout, b = t / g.Hout;
+    const int uy0 = oy * g.sh - g.ph, ux0 = ox * g.sw - g.pw;
+    const bf16* xb = x + static_cast<int64_t>(b) * g.Hin * g.Win * g.Cin;
+    bf16* dst = cols + static_cast<int64_t>(m) * (chunks * 8);
+    for (int j = sub; j < chunks; j += lanes) {
+      const int tap = j >> c8_shift, c8 = j - (tap << c8_shift);
+      const int kh = tap / KW, kw = tap - kh * KW;
+      const int uy = uy0 + kh, ux = ux0 + kw;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (uy >= 0 && ux >= 0 && uy < Hup && ux < Wup)
+        v = *reinterpret_cast<const uint4*>(xb + (static_cast<int64_t>(uy / UP) * g.Win + ux / UP) * g.Cin + c8 * 8);
+      *reinterpret_cast<uint4*>(dst + j * 8) = v;
     }
   }
 }
@@ -678,8 +720,9 @@ __global__ void bias_grad_kernel(const bf16* __restrict__ dpre, int64_t ld, int6
 
 // Column sums with 16-byte loads (C % 8 == 0, ld % 8 == 0, aligned base): a
 // CTA sums a slab of rows; L threads span a row's column groups of 8, R = 256
-// / L rows are read at once, and the R partial sums of a column group meet in
-// shared memory before one atomic per column and CTA.
+// / L rows are read at once (four loads in flight per thread), and the R
+// partial sums of each column meet in shared memory, summed by 256 threads in
+// parallel, before one atomic per column and CTA.
 __global__ void __launch_bounds__(256) bias_grad_v8_kernel(const bf16* __restrict__ dpre, int64_t ld, int64_t M,
                                                            int C, int64_t rows_per_cta, float* __restrict__ db) {
   __shared__ float red[256 * 8];
@@ -691,6 +734,7 @@ __global__ void __launch_bounds__(256) bias_grad_v8_kernel(const bf16* __restric
     const int cg = cg0 + cgi;
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (rr < R && cg < G) {
+#pragma unroll 4
       for (int64_t r = r0 + rr; r < r1; r += R) {
         const uint4 v = *reinterpret_cast<const uint4*>(dpre + r * ld + cg * 8);
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
@@ -701,22 +745,17 @@ __global__ void __launch_bounds__(256) bias_grad_v8_kernel(const bf16* __restric
         }
       }
     }
-    if (R > 1) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) red[t * 8 + j] = acc[j];
-      __syncthreads();
-      if (rr == 0 && cg < G) {
-        for (int q = 1; q < R; ++q)
-#pragma unroll
-          for (int j = 0; j < 8; ++j) acc[j] += red[(q * L + cgi) * 8 + j];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) atomicAdd(db + cg * 8 + j, acc[j]);
-      }
-      __syncthreads();
-    } else if (cg < G) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) atomicAdd(db + cg * 8 + j, acc[j]);
+    for (int j = 0; j < 8; ++j) red[t * 8 + j] = acc[j];
+    __syncthreads();
+    for (int q = t; q < L * 8; q += 256) {   // q = column group within the pass x 8 + column
+      const int qc = q >> 3, j = q & 7;
+      if (cg0 + qc >= G) continue;
+      float sum = 0.f;
+      for (int p = 0; p < R; ++p) sum += red[(p * L + qc) * 8 + j];
+      atomicAdd(db + (cg0 + qc) * 8 + j, sum);
     }
+    __syncthreads();
   }
 }
 
@@ -1098,7 +1137,28 @@ int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t t
   if (transposed)
     im2col_t_kernel<<<grid_for_l(M * K), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, ldt, static_cast<bf16*>(cols));
   else if (g.Cin % 8 == 0 && Kc == K && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
-           (reinterpret_cast<uintptr_t>(cols) & 15) == 0)
+           (reinterpret_cast<uintptr_t>(cols) & 15) == 0 && (g.Cin & (g.Cin - 1)) == 0 && M * K / 8 < (1LL << 31) &&
+           static_cast<long long>(g.B) * g.Hin * g.Win * g.Cin < (1LL << 31)) {
+    int c8_shift = 0;
+    while ((8 << c8_shift) < g.Cin) ++c8_shift;
+    const int chunks = K / 8;
+    int lanes_shift = 0;
+    while ((1 << lanes_shift) < chunks && lanes_shift < 5) ++lanes_shift;
+    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(
+        (M * (1LL << lanes_shift) + 255) / 256, 148LL * 32)));
+    const bf16* xx = static_cast<const bf16*>(x);
+    bf16* cc = static_cast<bf16*>(cols);
+    const int m = static_cast<int>(M);
+    if (g.KW == 1 && g.up == 1)
+      im2col_px_kernel<1, 1><<<grid, 256, 0, st>>>(xx, g, m, chunks, c8_shift, lanes_shift, cc);
+    else if (g.KW == 3 && g.up == 1)
+      im2col_px_kernel<3, 1><<<grid, 256, 0, st>>>(xx, g, m, chunks, c8_shift, lanes_shift, cc);
+    else if (g.KW == 3 && g.up == 2)
+      im2col_px_kernel<3, 2><<<grid, 256, 0, st>>>(xx, g, m, chunks, c8_shift, lanes_shift, cc);
+    else
+      im2col_px_kernel<0, 0><<<grid, 256, 0, st>>>(xx, g, m, chunks, c8_shift, lanes_shift, cc);
+  } else if (g.Cin % 8 == 0 && Kc == K && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+             (reinterpret_cast<uintptr_t>(cols) & 15) == 0)
     im2col_vec8_kernel<<<grid_for_l(M * K / 8), 256, 0, st>>>(static_cast<const bf16*>(x), g, static_cast<bf16*>(cols));
   else if (Kc % 8 == 0 && Kc <= 96 && (reinterpret_cast<uintptr_t>(cols) & 15) == 0)
     im2col_rows_kernel<<<static_cast<int>(std::min<long long>((M + kRowThreads - 1) / kRowThreads, 148LL * 8)),
@@ -1162,9 +1222,28 @@ int32_t ss_col2im16_lrelu_bf16(const void* dcols, const int32_t* conv, int32_t K
     return fail(SS_ERR_UNSUPPORTED, "BF16 column gradients need Cin % 8 == 0, Kc % 8 == 0 and 16-byte aligned buffers");
   const long long total = static_cast<long long>(g.B) * g.Hin * g.Win * (g.Cin / 8);
   if (total >= (1LL << 31)) return fail(SS_ERR_UNSUPPORTED, "too many input elements for one launch");
-  col2im16_lrelu_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const bf16*>(dcols), g, Kc, static_cast<const bf16*>(y), slope, static_cast<bf16*>(dpre), ldp,
-      static_cast<int>(total));
+  int c8_shift = 0;
+  while ((8 << c8_shift) < g.Cin) ++c8_shift;
+  if ((8 << c8_shift) != g.Cin) return fail(SS_ERR_UNSUPPORTED, "BF16 column gradients need Cin / 8 a power of two");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int grid = grid_for_l(total);
+  const bf16* dc = static_cast<const bf16*>(dcols);
+  const bf16* yy = static_cast<const bf16*>(y);
+  bf16* dp = static_cast<bf16*>(dpre);
+  const int n = static_cast<int>(total);
+  auto is = [&](int kh, int kw, int sh, int sw, int up) {
+    return g.KH == kh && g.KW == kw && g.sh == sh && g.sw == sw && g.up == up;
+  };
+  if (is(4, 1, 2, 1, 1))
+    col2im16_lrelu_kernel<4, 1, 2, 1, 1><<<grid, 256, 0, st>>>(dc, g, Kc, yy, slope, dp, ldp, n, c8_shift);
+  else if (is(3, 3, 2, 2, 1))
+    col2im16_lrelu_kernel<3, 3, 2, 2, 1><<<grid, 256, 0, st>>>(dc, g, Kc, yy, slope, dp, ldp, n, c8_shift);
+  else if (is(3, 3, 1, 1, 2))
+    col2im16_lrelu_kernel<3, 3, 1, 1, 2><<<grid, 256, 0, st>>>(dc, g, Kc, yy, slope, dp, ldp, n, c8_shift);
+  else if (is(1, 1, 1, 1, 1))
+    col2im16_lrelu_kernel<1, 1, 1, 1, 1><<<grid, 256, 0, st>>>(dc, g, Kc, yy, slope, dp, ldp, n, c8_shift);
+  else
+    col2im16_lrelu_kernel<0, 0, 0, 0, 0><<<grid, 256, 0, st>>>(dc, g, Kc, yy, slope, dp, ldp, n, c8_shift);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }
@@ -1222,7 +1301,7 @@ int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, fl
   if (!dpre || !db || M < 1 || C < 1 || ld < C) return fail(SS_ERR_INVALID, "bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (C % 8 == 0 && ld % 8 == 0 && (reinterpret_cast<uintptr_t>(dpre) & 15) == 0) {
-    const long long ctas = std::max(1LL, std::min((static_cast<long long>(M) + 255) / 256, 148LL * 8));
+    const long long ctas = std::max(1LL, std::min((static_cast<long long>(M) + 255) / 256, 148LL * 4));
     const long long rows = (M + ctas - 1) / ctas;
     bias_grad_v8_kernel<<<static_cast<unsigned>((M + rows - 1) / rows), 256, 0, st>>>(static_cast<const bf16*>(dpre),
                                                                                       ld, M, C, rows, db);

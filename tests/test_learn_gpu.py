@@ -193,3 +193,60 @@ def test_adamw_step_and_training_reduces_loss():
         losses.append(net.loss_sum.item() / (B * 70 * 70))
     net.check()
     assert losses[-1] < 0.5 * losses[0]
+
+
+# (B, Hin, Win, Cin, KH, KW, sh, sw, ph, pw, up): the network's three layer families, a 1x1 layer, a geometry
+# that takes the run-time-geometry kernels (KW = 2, upsampling by 3) and one whose Cin / 8 is not a power of two
+CONV_CASES = [(2, 50, 14, 32, 4, 1, 2, 1, 1, 0, 1), (2, 31, 13, 64, 3, 3, 2, 2, 1, 1, 1),
+              (2, 10, 9, 16, 3, 3, 1, 1, 1, 1, 2), (3, 1, 1, 128, 1, 1, 1, 1, 0, 0, 1),
+              (2, 7, 6, 8, 2, 3, 1, 2, 0, 1, 3), (2, 9, 11, 24, 3, 3, 1, 1, 1, 1, 1)]
+
+
+def _unfold_cols(x, conv):
+    """Columns [pixels][(kh, kw, c)] of NHWC x (float), through torch's unfold on the upsampled map."""
+    import torch.nn.functional as F
+    B, H, W, C, KH, KW, sh, sw, ph, pw, up = conv
+    xin = x.permute(0, 3, 1, 2)
+    if up > 1:
+        xin = F.interpolate(xin, scale_factor=up, mode='nearest')
+    u = F.unfold(xin, (KH, KW), padding=(ph, pw), stride=(sh, sw))
+    return u.view(B, C, KH * KW, -1).permute(0, 3, 2, 1).reshape(-1, KH * KW * C)
+
+
+@pytest.mark.parametrize('conv', CONV_CASES)
+def test_im2col_matches_unfold(conv):
+    """ss_im2col_bf16 copies: bit-exact against torch's unfold in the kernel's (kh, kw, c) column order."""
+    import ctypes
+    from shotsweep_b200 import _lib
+    B, H, W, C = conv[:4]
+    g = torch.Generator(device='cuda').manual_seed(sum(conv))
+    x = torch.randn(B, H, W, C, device='cuda', generator=g).to(torch.bfloat16)
+    ref = _unfold_cols(x.float(), conv)
+    cols = torch.full_like(ref, float('nan'), dtype=torch.bfloat16)
+    L = _lib.load()
+    _lib.check(L.ss_im2col_bf16(_lib.ptr(x), (ctypes.c_int32 * 11)(*conv), ref.shape[1], 0, 0, _lib.ptr(cols),
+                                _lib.stream_handle(x.device)), 'ss_im2col_bf16')
+    torch.cuda.synchronize()
+    assert torch.equal(cols.float(), ref)
+
+
+@pytest.mark.parametrize('conv', [c for c in CONV_CASES if c[3] % 8 == 0 and (c[3] // 8) & (c[3] // 8 - 1) == 0])
+def test_col2im16_matches_fold(conv):
+    """ss_col2im16_lrelu_bf16: BF16 column gradients summed back onto the input in float32 (torch's fold, then the
+    upsampling's adjoint), times the leaky-ReLU derivative of y, one BF16 rounding: within one BF16 unit."""
+    import ctypes
+    from shotsweep_b200 import _lib
+    B, H, W, C = conv[:4]
+    g = torch.Generator(device='cuda').manual_seed(7 + sum(conv))
+    x = torch.randn(B, H, W, C, device='cuda', generator=g).to(torch.bfloat16)
+    xr = x.float().requires_grad_(True)
+    cols = _unfold_cols(xr, conv)
+    dcols = torch.randn(cols.shape, device='cuda', generator=g).to(torch.bfloat16)
+    cols.backward(dcols.float())
+    ref = torch.where(x.float() > 0, xr.grad, 0.2 * xr.grad)
+    out = torch.full_like(x, float('nan'))
+    L = _lib.load()
+    _lib.check(L.ss_col2im16_lrelu_bf16(_lib.ptr(dcols), (ctypes.c_int32 * 11)(*conv), cols.shape[1], _lib.ptr(x),
+                                        0.2, _lib.ptr(out), C, _lib.stream_handle(x.device)), 'ss_col2im16_lrelu_bf16')
+    torch.cuda.synchronize()
+    assert ((out.float() - ref).abs() <= 2 ** -8 * ref.abs() + 1e-6).all()
