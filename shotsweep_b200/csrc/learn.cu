@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(256) bias_grad_v8_kernel(const bf16* __restric
   const int t = threadIdx.x, cgi = t % L, rr = t / L;
   const int64_t r0 = blockIdx.x * rows_per_cta;
   const int64_t r1 = r0 + rows_per_cta < M ? r0 + rows_per_cta : M;
-  for (int cg0 = 0; cg0 < G; cg0 += L) {
+  for (int cg0 = blockIdx.y * L; cg0 < G; cg0 += gridDim.y * L) {
     const int cg = cg0 + cgi;
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (rr < R && cg < G) {
@@ -1090,7 +1090,7 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
   // tile width: the smallest of 32 / 64 / 128 covering N, 256 for wide outputs with enough row tiles
   int bn = N <= 32 && !bmn ? 32 : N <= 64 ? 64 : 128;
   const int m_tiles = (M + kBM - 1) / kBM;
-  if (N >= 256 && m_tiles * ((N + 255) / 256) >= 148) bn = 256;
+  if (N >= 256 && m_tiles * ((N + 255) / 256) >= 148 && k_tiles > 2) bn = 256;   // short K: 128-wide tiles, 4 CTAs per SM
   const int tiles = m_tiles * ((N + bn - 1) / bn);
   if (splits <= 0) {   // split the K loop only where the output is accumulated, to fill the GPU
     splits = 1;
@@ -1301,10 +1301,12 @@ int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, fl
   if (!dpre || !db || M < 1 || C < 1 || ld < C) return fail(SS_ERR_INVALID, "bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (C % 8 == 0 && ld % 8 == 0 && (reinterpret_cast<uintptr_t>(dpre) & 15) == 0) {
-    const long long ctas = std::max(1LL, std::min((static_cast<long long>(M) + 255) / 256, 148LL * 4));
+    // column passes of 256 groups across grid.y; row slabs of at least 32 rows across grid.x
+    const int G = C / 8, passes = (G + 255) / 256;
+    const long long ctas = std::max(1LL, std::min((static_cast<long long>(M) + 31) / 32, 148LL * 4 / passes + 1));
     const long long rows = (M + ctas - 1) / ctas;
-    bias_grad_v8_kernel<<<static_cast<unsigned>((M + rows - 1) / rows), 256, 0, st>>>(static_cast<const bf16*>(dpre),
-                                                                                      ld, M, C, rows, db);
+    bias_grad_v8_kernel<<<dim3(static_cast<unsigned>((M + rows - 1) / rows), passes), 256, 0, st>>>(
+        static_cast<const bf16*>(dpre), ld, M, C, rows, db);
   } else {
     dim3 grid((C + 127) / 128, static_cast<unsigned>(std::min<long long>(M, 512)));
     bias_grad_kernel<<<grid, 128, 0, st>>>(static_cast<const bf16*>(dpre), ld, M, C, db);
