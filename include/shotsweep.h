@@ -219,9 +219,9 @@ int32_t ss_c2_field(const ss_geometry* geom, int32_t n_models, const float* vel,
  *     SS_ERR_UNSUPPORTED; the 70x70 / 1000-step OpenFWI geometry needs about
  *     90 MB per solve and so needs ss_images.  Smaller problems run with as
  *     many solves in flight as fit in the array.
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *   - The call cannot be captured into a CUDA graph: it ends by waiting for
+ *     its work (below), and returns SS_ERR_UNSUPPORTED when `stream` is
+ *     capturing.
  *   - Every call shares the one array, and it keeps the previous call's
  *     contents: calls that overlap on the GPU (other streams, other host
  *     threads) race and corrupt each other's results.

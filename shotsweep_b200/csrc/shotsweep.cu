@@ -2317,22 +2317,30 @@ int32_t ss_images_noalloc(const ss_geometry* geom, int32_t n_models, const float
   if (n_models < 1) return fail(SS_ERR_INVALID, "n_models must be positive");
   if (!vel || !wavelet || !obs || !illum || !img) return fail(SS_ERR_INVALID, "vel, wavelet, obs, img and illum are required");
   if (!(eps > 0.f)) return fail(SS_ERR_INVALID, "illumination regularization eps must be positive");
+  {
+    // the call ends by waiting for its own work, which a stream capture cannot record
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    SS_CUDA(cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(SS_ERR_UNSUPPORTED, "ss_images_noalloc waits for its work and cannot be captured into a CUDA graph");
+  }
   void* scratch = nullptr;
   rc = noalloc_scratch(&scratch);
   if (rc) return rc;
   Plan p;
   rc = make_plan(geom, SS_MODE_IMAGES, n_models * geom->n_shots, &p);
   if (rc) return rc;
-  // Fewer solves in flight until their scratch fits the fixed array.
-  WsLayout L = ws_layout(geom, p, SS_MODE_IMAGES);
-  while (L.total > kNoAllocScratchBytes && p.slots > 1) {
-    --p.slots;
-    L = ws_layout(geom, p, SS_MODE_IMAGES);
-  }
-  if (L.total > kNoAllocScratchBytes)
-    return fail(SS_ERR_UNSUPPORTED, "one solve of this geometry needs " + std::to_string(L.total) +
+  // As many solves in flight as their scratch fits in the fixed array.
+  const int fit = slots_for_bytes(geom, p, SS_MODE_IMAGES, kNoAllocScratchBytes);
+  if (fit < 1) {
+    p.slots = 1;
+    return fail(SS_ERR_UNSUPPORTED, "one solve of this geometry needs " +
+                                        std::to_string(ws_layout(geom, p, SS_MODE_IMAGES).total) +
                                         " bytes of scratch, more than the 33554432-byte allocation-free array; "
                                         "use ss_images with a workspace");
+  }
+  p.slots = std::min(p.slots, fit);
+  const WsLayout L = ws_layout(geom, p, SS_MODE_IMAGES);
   unsigned char* w = static_cast<unsigned char*>(scratch);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // The array keeps the previous call's contents; only the status word must

@@ -73,3 +73,29 @@ def test_noalloc_refuses_geometry_beyond_its_scratch():
                              _lib.ptr(out), _lib.ptr(out.clone()), None, _lib.stream_handle(dev))
     assert rc == _lib.ERR_UNSUPPORTED
     assert b'scratch' in L.ss_last_error()
+
+
+def test_noalloc_refuses_stream_capture():
+    """The call ends by waiting for its own work, which a CUDA graph cannot record: on a capturing stream it
+    returns SS_ERR_UNSUPPORTED before it enqueues anything, and the capture ends cleanly."""
+    from shotsweep_b200 import _lib, engine
+    geom = engine.geometry(23, 37, 160, 9, (0, 18, 36))
+    dev = torch.device('cuda', torch.cuda.current_device())
+    L = _lib.load()
+    x = torch.zeros(1, 3, 160, 37, device=dev)
+    v = torch.full((1, 23, 37), 2000.0, device=dev)
+    w = torch.zeros(160, device=dev)
+    img = torch.empty(1, 3, 23, 37, device=dev)
+    illum = torch.empty_like(img)
+    side = torch.cuda.Stream(dev)
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(side):
+        graph.capture_begin()
+        try:
+            rc = L.ss_images_noalloc(ctypes.byref(geom), 1, _lib.ptr(v), _lib.ptr(w), _lib.ptr(x), None, 0.03, 1e-4,
+                                     1, _lib.ptr(img), _lib.ptr(illum), None, ctypes.c_void_p(side.cuda_stream))
+        finally:
+            graph.capture_end()
+    assert rc == _lib.ERR_UNSUPPORTED
+    assert b'captured' in L.ss_last_error()
