@@ -1038,6 +1038,35 @@ __global__ void adamw_kernel(float* __restrict__ p, const float* __restrict__ gr
 
 // Network input: stored float16 gathers [n][S][T][X] of the samples ids[0..B)
 // as BF16 NHWC [B][T][X][S] divided by the normalisation scale.
+// One thread per (model, t, x) pixel: its S <= 8 samples come from S planes
+// of the stored gathers (each plane read coalesced across the warp); a
+// block's 256 x S outputs leave through shared memory as 16-byte stores.
+// 32-bit pixel indices (the host checks the count).
+__global__ void __launch_bounds__(256) gathers_nhwc_px_kernel(const uint16_t* __restrict__ stored,
+                                                              const int* __restrict__ ids, int S, int T, int X,
+                                                              float scale, bf16* __restrict__ out, int total_px) {
+  __shared__ __align__(16) bf16 buf[256 * 8];
+  const int64_t plane = static_cast<int64_t>(T) * X;
+  for (int p0 = blockIdx.x * 256; p0 < total_px; p0 += gridDim.x * 256) {
+    const int p = p0 + threadIdx.x;
+    if (p < total_px) {
+      const int x = p % X, bt = p / X;
+      const int t = bt % T, b = bt / T;
+      const uint16_t* src = stored + static_cast<int64_t>(ids[b]) * S * plane + static_cast<int64_t>(t) * X + x;
+      for (int s = 0; s < S; ++s)
+        buf[threadIdx.x * S + s] =
+            __float2bfloat16_rn(__fdiv_rn(__half2float(__ushort_as_half(src[s * plane])), scale));
+    }
+    __syncthreads();
+    const int n = min(256, total_px - p0) * S;   // this block's outputs, from a 16-byte aligned start
+    bf16* dst = out + static_cast<int64_t>(p0) * S;
+    for (int j = threadIdx.x; j < n / 8; j += 256)
+      reinterpret_cast<uint4*>(dst)[j] = reinterpret_cast<const uint4*>(buf)[j];
+    for (int j = (n / 8) * 8 + threadIdx.x; j < n; j += 256) dst[j] = buf[j];
+    __syncthreads();
+  }
+}
+
 __global__ void gathers_nhwc_kernel(const uint16_t* __restrict__ stored, const int* __restrict__ ids, int B, int S,
                                     int T, int X, float scale, bf16* __restrict__ out) {
   const int64_t total = static_cast<int64_t>(B) * T * X * S;
@@ -1393,6 +1422,14 @@ int32_t ss_gathers_nhwc_bf16(const uint16_t* stored, const int32_t* ids, int32_t
   if (!stored || !ids || !out || B < 1 || S < 1 || T < 1 || X < 1) return fail(SS_ERR_INVALID, "bad arguments");
   if (!std::isfinite(scale) || !(scale > 0.f)) return fail(SS_ERR_INVALID, "Gather normalization scale must be finite and positive");
   const long long total = static_cast<long long>(B) * S * T * X;
+  const long long px = static_cast<long long>(B) * T * X;
+  if (S <= 8 && px < (1LL << 31) && (reinterpret_cast<uintptr_t>(out) & 15) == 0) {
+    const int grid = static_cast<int>(std::min<long long>((px + 255) / 256, 148LL * 8));
+    gathers_nhwc_px_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        stored, ids, S, T, X, scale, static_cast<bf16*>(out), static_cast<int>(px));
+    SS_TRY_CUDA(cudaGetLastError());
+    return SS_OK;
+  }
   gathers_nhwc_kernel<<<grid_for_l(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(stored, ids, B, S, T, X, scale,
                                                                                        static_cast<bf16*>(out));
   SS_TRY_CUDA(cudaGetLastError());

@@ -250,3 +250,23 @@ def test_col2im16_matches_fold(conv):
                                         0.2, _lib.ptr(out), C, _lib.stream_handle(x.device)), 'ss_col2im16_lrelu_bf16')
     torch.cuda.synchronize()
     assert ((out.float() - ref).abs() <= 2 ** -8 * ref.abs() + 1e-6).all()
+
+
+@pytest.mark.parametrize('S,T,X,B', [(5, 37, 70, 6), (9, 11, 13, 3)])
+def test_gathers_nhwc_matches_restatement(S, T, X, B):
+    """ss_gathers_nhwc_bf16: rows `ids` of stored float16 gathers [n][S][T][X], divided by the scale (correctly
+    rounded, as torch divides) and rounded to BF16, as NHWC [B][T][X][S]: bit-exact (S = 5 takes the pixel-per-thread
+    kernel with shared-memory staged stores, S = 9 the element-per-thread one)."""
+    from shotsweep_b200 import _lib
+    g = torch.Generator(device='cuda').manual_seed(S * T + X)
+    n = B + 4
+    stored = (torch.randn(n, S, T, X, device='cuda', generator=g) * 300).to(torch.float16)
+    ids = torch.randperm(n, device='cuda', generator=g)[:B].to(torch.int32)
+    scale = 123.456
+    ref = (stored[ids.long()].float() / scale).permute(0, 2, 3, 1).to(torch.bfloat16)
+    out = torch.full((B, T, X, S), float('nan'), device='cuda', dtype=torch.bfloat16)
+    L = _lib.load()
+    _lib.check(L.ss_gathers_nhwc_bf16(_lib.ptr(stored), _lib.ptr(ids), B, S, T, X, scale, _lib.ptr(out),
+                                      _lib.stream_handle(out.device)), 'ss_gathers_nhwc_bf16')
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
