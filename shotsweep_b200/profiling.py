@@ -3,7 +3,12 @@
     python -m shotsweep_b200.profiling [n_models]
     python -m shotsweep_b200.profiling learned [batch]
     python -m shotsweep_b200.profiling uneven [solves]
+    python -m shotsweep_b200.profiling uneven-classes [CxR ...]
     python -m shotsweep_b200.profiling gemm
+
+`uneven-classes` times every size class of the uneven bench workload (2000 solves, full time axes) alone at its
+tuned launch shape and at the extra (cluster x rows per thread) shapes given, then the whole batch under each
+stream schedule.
 
 The last form times the tensor-core GEMM on square BF16 problems (4096^3, 8192^3; BF16 and F32 outputs)
 beside torch.matmul on the same device.
@@ -109,6 +114,52 @@ def uneven(n_solves=48):
           f'images {e0.elapsed_time(e1):.3f} ms')
 
 
+def uneven_classes(extra=(), n_solves=2000, seed=2):
+    """Per-class CUDA-event times of the uneven bench workload (see the module docstring)."""
+    from . import autotune
+    from .batch import Shape, UnevenBatch
+    dev = torch.device('cuda', torch.cuda.current_device())
+    shapes = []
+    for m in synth.uneven_workload(n_solves, seed=seed):
+        nz, nx = m['truth'].shape
+        shapes += [Shape(nz, nx, m['nt'], m['shot_cols'], v_mute=m['v_s']) for _ in m['backgrounds']]
+    table = autotune.tune(shapes, device=dev)
+    total = 0.0
+    for c_min, idx in sorted(autotune.class_members(shapes).items()):
+        sub = [shapes[i] for i in idx]
+        for shape in [table[c_min]] + [s for s in extra if s != table[c_min]]:
+            try:
+                secs, work = autotune._time_class(sub, shape, c_min, dev, 10 ** 6, 2)
+            except RuntimeError:      # the class does not fit this launch shape
+                continue
+            b = UnevenBatch(sub, device=dev, clusters={c_min: shape}, schedule=0)
+            inflight = sum(c['slots'] for c in b.classes())
+            del b
+            total += secs if shape == table[c_min] else 0.0
+            print(f'class {c_min:2d} {"tuned" if shape == table[c_min] else "other"} {shape}: {len(sub)} rows, '
+                  f'{sum(s.n_shots for s in sub)} solves, {inflight} in flight, {secs * 1e3:.1f} ms, '
+                  f'{work / secs / 1e9:.1f} Gcell-steps/s, {work / secs / 1e9 / (inflight * shape[0]):.2f} per SM',
+                  flush=True)
+    print(f'sum over classes at the tuned shapes: {total * 1e3:.1f} ms')
+    rng = np.random.default_rng(0)
+    for sched in UnevenBatch.SCHEDULES:
+        b = UnevenBatch(shapes, device=dev, clusters=table, schedule=sched)
+        vel = b.pack_models([np.full((s.nz, s.nx), 2500.0, np.float32) for s in shapes])
+        obs = b.pack_traces([rng.standard_normal((s.n_shots, s.nt, s.nx)).astype(np.float32) for s in shapes])
+        w = torch.zeros(b.max_nt, dtype=torch.float32, device=dev)
+        w[:40] = 1.0
+        out = (b._empty(b.n_out), b._empty(b.n_out), None)
+        b.images(vel, w, obs, out=out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.images(vel, w, obs, out=out)
+        e1.record()
+        e1.synchronize()
+        b.status()
+        print(f'whole batch, schedule {sched}: {e0.elapsed_time(e1):.1f} ms')
+        del b, vel, obs, out
+
+
 def gemm():
     from . import _lib
     L = _lib.load()
@@ -147,6 +198,8 @@ if __name__ == '__main__':
         learned(int(sys.argv[2]) if len(sys.argv) > 2 else 64)
     elif len(sys.argv) > 1 and sys.argv[1] == 'gemm':
         gemm()
+    elif len(sys.argv) > 1 and sys.argv[1] == 'uneven-classes':
+        uneven_classes(tuple(tuple(int(v) for v in a.split('x')) for a in sys.argv[2:]))
     elif len(sys.argv) > 1 and sys.argv[1] == 'uneven':
         uneven(int(sys.argv[2]) if len(sys.argv) > 2 else 48)
     else:
