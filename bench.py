@@ -368,7 +368,7 @@ def run_ours(args):
     roofline = {'bound': 'fp32', 'achieved': achieved, 'peak': peak, 'unit': 'TFLOP/s', 'frac': achieved / peak,
                 'traffic': per_solve * shot_images if per_solve else None,
                 'peak_source': 'measured live: max of scalar FFMA and packed FFMA2 probes on all SMs '
-                               '(MEASURED_PEAKS.json has no FP32 figure)',
+                               '(the measured HBM and BF16 peaks carry no FP32 figure)',
                 'algorithmic': '36 flops per padded cell per step (16 forward + 20 adjoint), 150^2 cells, 1000 steps; '
                                'traffic = ncu dram read + write bytes per solve x solves',
                 'traffic_source': traffic_src,
