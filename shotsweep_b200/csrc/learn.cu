@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -55,9 +56,12 @@ constexpr size_t gemm_smem_bytes(int stages = kStagesG) {
 
 // AMN / BMN: operand stored K-outer (A[k][m], B[k][n]) and read in place
 // through MN-major descriptors, two (A) or BN/64 (B) 64 x 64 boxes per stage.
-template <int BN, int EPI, bool AMN, bool BMN>
+// TMAC (BF16 epilogue only): C leaves through TMA tile stores (map tc: boxes
+// of 32 x 32, 64-byte swizzle) instead of per-thread stores.
+template <int BN, int EPI, bool AMN, bool BMN, bool TMAC>
 __global__ void __launch_bounds__(kGemmThreads, 1)
-    gemm_bf16_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, const GemmArgs g) {
+    gemm_bf16_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+                     const __grid_constant__ CUtensorMap tc, const GemmArgs g) {
   using namespace sm100;
   constexpr uint32_t A_BYTES = kBM * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
   constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
@@ -138,6 +142,53 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     mbar_wait(acc_bar, 0, g.err, 3);
     tc_fence_after();
     const int q = warp & 3;
+    if constexpr (TMAC) {
+      // Two 2 KB BF16 slabs per warp in stage 0 (1024-byte aligned), alternated
+      // so that a slab's previous store has read it before it is rewritten.
+      // Row r (this lane) holds 32 columns = four 16-byte chunks; chunk j sits
+      // at chunk j ^ ((r >> 1) & 3) of the row, the 64-byte swizzle the map
+      // uses, which also spreads the warp's writes over all banks.
+      const uint32_t slab0 = sbase + static_cast<uint32_t>(q) * 4096u;
+      int k = 0;
+#pragma unroll 1
+      for (int c = 0; c < BN && n0 + c < g.N; c += 32, ++k) {
+        float v[32];
+        tmem_ld32(taddr + (static_cast<uint32_t>(q * 32) << 16) + c, v);
+        uint32_t pk[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          float x0 = v[2 * j], x1 = v[2 * j + 1];
+          if (g.bias) {
+            const int col = n0 + c + 2 * j;
+            x0 += col < g.N ? g.bias[col] : 0.f;
+            x1 += col + 1 < g.N ? g.bias[col + 1] : 0.f;
+          }
+          x0 = x0 > 0.f ? x0 : g.slope * x0;
+          x1 = x1 > 0.f ? x1 : g.slope * x1;
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+          pk[j] = *reinterpret_cast<const uint32_t*>(&h);
+        }
+        const uint32_t slab = slab0 + static_cast<uint32_t>(k & 1) * 2048u;
+        if (lane == 0) bulk_wait_read<1>();   // the store issued from this slab two slabs ago has read it
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t a =
+              slab + static_cast<uint32_t>(lane) * 64u + static_cast<uint32_t>((j ^ ((lane >> 1) & 3)) * 16);
+          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(pk[4 * j]), "r"(pk[4 * j + 1]),
+                       "r"(pk[4 * j + 2]), "r"(pk[4 * j + 3])
+                       : "memory");
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          tma_store_2d(&tc, slab, n0 + c, m0 + q * 32);
+          bulk_commit();
+        }
+      }
+      if (lane == 0) bulk_wait_all();
+      __syncwarp();
+    } else {
     float* slab = reinterpret_cast<float*>(base) + q * (32 * 33);
     const int rsub = lane >> 3, c4 = (lane & 7) * 4;
     const bool vec = g.ldc % 4 == 0;
@@ -195,6 +246,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       }
       __syncwarp();
     }
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -219,6 +271,22 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+// BF16 output matrix [rows][ld] (first `cols` columns) as TMA store tiles of
+// 32 x 32 with the 64-byte swizzle (the epilogue's slab layout).
+int make_tmap_store(CUtensorMap* map, void* ptr, long long cols, long long rows, long long ld) {
+  auto fn = encode_fn();
+  if (!fn) return fail(SS_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * 2)};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t es[2] = {1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(SS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
+  return SS_OK;
+}
+
 // K-major BF16 matrix [rows][ld] (K = first `k` columns) as TMA tiles of 64 x box_rows.
 int make_tmap(CUtensorMap* map, const void* ptr, long long k, long long rows, long long ld, int box_rows) {
   auto fn = encode_fn();
@@ -236,9 +304,10 @@ int make_tmap(CUtensorMap* map, const void* ptr, long long k, long long rows, lo
   return SS_OK;
 }
 
-template <int BN, int EPI, bool AMN, bool BMN>
-int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits, cudaStream_t st) {
-  auto kern = gemm_bf16_kernel<BN, EPI, AMN, BMN>;
+template <int BN, int EPI, bool AMN, bool BMN, bool TMAC = false>
+int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tc, const GemmArgs& g, int splits,
+                  cudaStream_t st) {
+  auto kern = gemm_bf16_kernel<BN, EPI, AMN, BMN, TMAC>;
   constexpr size_t smem = gemm_smem_bytes<BN>();   // the attribute allows the full ring
   const size_t smem_run = gemm_smem_bytes<BN>(g.stages);
   // the attribute is per device: set once on each device that launches this instantiation
@@ -255,32 +324,35 @@ int launch_gemm_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& 
     }
   }
   dim3 grid((g.N + BN - 1) / BN, (g.M + kBM - 1) / kBM, splits);
-  kern<<<grid, kGemmThreads, smem_run, st>>>(ta, tb, g);
+  kern<<<grid, kGemmThreads, smem_run, st>>>(ta, tb, tc, g);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }
 
+// tc: the output's store map when `tmac` (BF16 epilogue with a stride TMA can describe), else unused.
 template <int BN, bool AMN, bool BMN>
-int launch_gemm_epi(int epi, const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits,
-                    cudaStream_t st) {
+int launch_gemm_epi(int epi, bool tmac, const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tc,
+                    const GemmArgs& g, int splits, cudaStream_t st) {
   switch (epi) {
-    case SS_EPI_F32: return launch_gemm_t<BN, SS_EPI_F32, AMN, BMN>(ta, tb, g, splits, st);
-    case SS_EPI_F32_ADD: return launch_gemm_t<BN, SS_EPI_F32_ADD, AMN, BMN>(ta, tb, g, splits, st);
-    case SS_EPI_BIAS_LRELU_BF16: return launch_gemm_t<BN, SS_EPI_BIAS_LRELU_BF16, AMN, BMN>(ta, tb, g, splits, st);
-    default: return launch_gemm_t<BN, SS_EPI_BIAS_F32, AMN, BMN>(ta, tb, g, splits, st);
+    case SS_EPI_F32: return launch_gemm_t<BN, SS_EPI_F32, AMN, BMN>(ta, tb, tc, g, splits, st);
+    case SS_EPI_F32_ADD: return launch_gemm_t<BN, SS_EPI_F32_ADD, AMN, BMN>(ta, tb, tc, g, splits, st);
+    case SS_EPI_BIAS_LRELU_BF16:
+      if (tmac) return launch_gemm_t<BN, SS_EPI_BIAS_LRELU_BF16, AMN, BMN, true>(ta, tb, tc, g, splits, st);
+      return launch_gemm_t<BN, SS_EPI_BIAS_LRELU_BF16, AMN, BMN>(ta, tb, tc, g, splits, st);
+    default: return launch_gemm_t<BN, SS_EPI_BIAS_F32, AMN, BMN>(ta, tb, tc, g, splits, st);
   }
 }
 
 // layout bit 0: A stored K-outer; bit 1: B stored K-outer (layouts 0, 2 and 3).
 // An MN-major B needs whole 64-column boxes, so its tiles are at least 64 wide.
 template <int BN>
-int launch_gemm_bn(int layout, int epi, const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& g, int splits,
-                   cudaStream_t st) {
+int launch_gemm_bn(int layout, int epi, bool tmac, const CUtensorMap& ta, const CUtensorMap& tb,
+                   const CUtensorMap& tc, const GemmArgs& g, int splits, cudaStream_t st) {
   if constexpr (BN >= 64) {
-    if (layout == 3) return launch_gemm_epi<BN, true, true>(epi, ta, tb, g, splits, st);
-    if (layout == 2) return launch_gemm_epi<BN, false, true>(epi, ta, tb, g, splits, st);
+    if (layout == 3) return launch_gemm_epi<BN, true, true>(epi, tmac, ta, tb, tc, g, splits, st);
+    if (layout == 2) return launch_gemm_epi<BN, false, true>(epi, tmac, ta, tb, tc, g, splits, st);
   }
-  return launch_gemm_epi<BN, false, false>(epi, ta, tb, g, splits, st);
+  return launch_gemm_epi<BN, false, false>(epi, tmac, ta, tb, tc, g, splits, st);
 }
 
 
@@ -1138,11 +1210,19 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
   if (rc) return rc;
   GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, std::min(kStagesG, per)};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // BF16 outputs whose rows TMA can address (16-byte aligned base and stride) leave through tile stores
+  CUtensorMap tc;
+  std::memset(&tc, 0, sizeof(tc));
+  const bool tmac = epi == SS_EPI_BIAS_LRELU_BF16 && ldc % 8 == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+  if (tmac) {
+    rc = make_tmap_store(&tc, C, N, M, ldc);
+    if (rc) return rc;
+  }
   switch (bn) {
-    case 32: return launch_gemm_bn<32>(layout, epi, ta, tb, g, splits, st);
-    case 64: return launch_gemm_bn<64>(layout, epi, ta, tb, g, splits, st);
-    case 128: return launch_gemm_bn<128>(layout, epi, ta, tb, g, splits, st);
-    default: return launch_gemm_bn<256>(layout, epi, ta, tb, g, splits, st);
+    case 32: return launch_gemm_bn<32>(layout, epi, tmac, ta, tb, tc, g, splits, st);
+    case 64: return launch_gemm_bn<64>(layout, epi, tmac, ta, tb, tc, g, splits, st);
+    case 128: return launch_gemm_bn<128>(layout, epi, tmac, ta, tb, tc, g, splits, st);
+    default: return launch_gemm_bn<256>(layout, epi, tmac, ta, tb, tc, g, splits, st);
   }
 }
 
