@@ -1210,10 +1210,13 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
   if (rc) return rc;
   GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, std::min(kStagesG, per)};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // BF16 outputs whose rows TMA can address (16-byte aligned base and stride) leave through tile stores
+  // BF16 outputs of one- or two-step K loops (epilogue-bound: the input-gradient GEMMs) leave through tile
+  // stores where TMA can address their rows (16-byte aligned base and stride); with longer K loops the
+  // per-thread stores timed faster inside the training step
   CUtensorMap tc;
   std::memset(&tc, 0, sizeof(tc));
-  const bool tmac = epi == SS_EPI_BIAS_LRELU_BF16 && ldc % 8 == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+  const bool tmac = epi == SS_EPI_BIAS_LRELU_BF16 && per <= 2 && ldc % 8 == 0 &&
+                    (reinterpret_cast<uintptr_t>(C) & 15) == 0;
   if (tmac) {
     rc = make_tmap_store(&tc, C, N, M, ldc);
     if (rc) return rc;
