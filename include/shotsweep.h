@@ -419,22 +419,13 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
  * KH, KW, stride_h, stride_w, pad_h, pad_w, up}: the input is read through a
  * nearest-neighbour upsampling by `up`; Hout = (Hin*up + 2 pad_h - KH) / stride_h + 1
  * (likewise W); column index k = (kh*KW + kw)*Cin + c.
- *   ss_im2col_bf16        cols [pixels][Kc] (k >= KH*KW*Cin zero), or with
- *                         `transposed` [KH*KW*Cin][ldt] (pixels innermost)
- *   ss_col2im_lrelu_bf16  dpre[pixel][c] (row stride ldp) = leaky_relu'(y) x the
- *                         sum of the column gradients dcols [pixels_out][Kc]
- *                         that read input element (pixel, c); y: the input map
- *   ss_col2im16_lrelu_bf16 the same with BF16 column gradients (Cin % 8 == 0,
- *                         Kc % 8 == 0, 16-byte aligned dcols and y; at most
- *                         2^31 - 1 input elements / 8)
- *   ss_im2col_both_bf16   cols [pixels][Kc] and, in the same pass, the columns
- *                         transposed [Kc][ldt] (Cin % 8 == 0, Kc == K): the
- *                         forward GEMM's operand and the weight gradient's
- *   ss_transpose_bf16     out[c][r] = in[r][c]
- *   ss_transpose_sum_bf16 the same, and colsum[c] += sum over rows of in[r][c]
- *                         in the same pass (a layer's bias gradient from its
- *                         pre-activation gradient while that is transposed for
- *                         the weight-gradient GEMM)
+ *   ss_im2col_bf16        cols [pixels][Kc] (k >= KH*KW*Cin zero)
+ *   ss_col2im16_lrelu_bf16 dpre[pixel][c] (row stride ldp) = leaky_relu'(y) x
+ *                         the sum of the BF16 column gradients dcols
+ *                         [pixels_out][Kc] that read input element (pixel, c);
+ *                         y: the input map (Cin % 8 == 0 with Cin / 8 a power
+ *                         of two, Kc % 8 == 0, 16-byte aligned dcols and y; at
+ *                         most 2^31 - 1 input elements / 8)
  *   ss_bias_grad_bf16     db[c] += sum over rows of dpre[row][c]
  * Output head: crop [off, off+n)^2 of x [B][H][W][C], 3x3 convolution with
  * zero padding, bias, tanh; head[6] = {B, H, W, C, off, n}; weights w[9][C].
@@ -446,17 +437,9 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
  * ss_gather_rows_f32      out[b][:] = src[ids[b]][:] (rows of `row` floats)
  * ss_gathers_nhwc_bf16    network input: stored float16 gathers [n][S][T][X] of
  *                         samples ids[0..B) as BF16 [B][T][X][S] / scale (3_train.py:198) */
-int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t transposed, int64_t ldt, void* cols,
-                       void* stream);
-int32_t ss_im2col_both_bf16(const void* x, const int32_t* conv, int32_t Kc, void* cols, void* colst, int64_t ldt,
-                            void* stream);
-int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
-                             void* dpre, int64_t ldp, void* stream);
+int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, void* cols, void* stream);
 int32_t ss_col2im16_lrelu_bf16(const void* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
                                void* dpre, int64_t ldp, void* stream);
-int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream);
-int32_t ss_transpose_sum_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out,
-                              float* colsum, void* stream);
 int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream);
 int32_t ss_head_forward(const void* x, const int32_t* head, const float* w, const float* bias, float* out, void* stream);
 int32_t ss_head_backward(const void* x, const int32_t* head, const float* w, const float* dpre, float slope, float* dw,

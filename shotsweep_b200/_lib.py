@@ -137,13 +137,8 @@ _SIGNATURES = {
     'ss_gemm_bf16_layout': (ctypes.c_int32, [_P, ctypes.c_int64, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int64, _P,
                                              ctypes.c_float, ctypes.c_int32, _P, _P]),
-    'ss_im2col_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _P, _P]),
-    'ss_im2col_both_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, _P, _P, ctypes.c_int64, _P]),
-    'ss_col2im_lrelu_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, _P, ctypes.c_float, _P, ctypes.c_int64, _P]),
+    'ss_im2col_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, _P, _P]),
     'ss_col2im16_lrelu_bf16': (ctypes.c_int32, [_P, _P, ctypes.c_int32, _P, ctypes.c_float, _P, ctypes.c_int64, _P]),
-    'ss_transpose_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int64, _P]),
-    'ss_transpose_sum_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _P, ctypes.c_int64,
-                                               _P, _P]),
     'ss_bias_grad_bf16': (ctypes.c_int32, [_P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _P, _P]),
     'ss_head_forward': (ctypes.c_int32, [_P, _P, _P, _P, _P, _P]),
     'ss_head_backward': (ctypes.c_int32, [_P, _P, _P, _P, ctypes.c_float, _P, _P, _P, _P]),

@@ -406,19 +406,6 @@ __global__ void im2col_vec8_kernel(const bf16* __restrict__ x, ConvGeom g, bf16*
   }
 }
 
-// The same columns transposed, [Kc][ldt] (pixels innermost), for weight gradients.
-__global__ void im2col_t_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int64_t ldt, bf16* __restrict__ colst) {
-  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
-  const int64_t total = M * K;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t m = i % M;
-    const int k = static_cast<int>(i / M);
-    const int64_t src = conv_src(g, m, k);
-    colst[static_cast<int64_t>(k) * ldt + m] = src >= 0 ? x[src] : __float2bfloat16_rn(0.f);
-  }
-}
-
 // Columns of small-K layers (K <= 64, Kc % 8 == 0; the first encoder layer,
 // whose 5 input channels rule out 16-byte gathers): each thread gathers one
 // pixel's row, tap by tap (runs of Cin contiguous inputs), into shared memory;
@@ -458,105 +445,6 @@ __global__ void __launch_bounds__(kRowThreads) im2col_rows_kernel(const bf16* __
   }
 }
 
-
-// Columns and their transpose in one pass (Cin % 8 == 0, K == Kc): a CTA
-// gathers a tile of 64 pixels x 64 column indices from the input map with
-// 16-byte loads into shared memory, writes the columns row by row (cols
-// [pixels][K], the forward GEMM's operand) and the same tile transposed
-// (colst [K][ldt], pixels innermost, the weight-gradient GEMM's operand), so
-// that the backward pass needs no transpose of the columns.
-__global__ void __launch_bounds__(256) im2col_both_kernel(const bf16* __restrict__ x, ConvGeom g, int K, int64_t ldt,
-                                                          bf16* __restrict__ cols, bf16* __restrict__ colst) {
-  __shared__ uint32_t tile[64][33];   // [pixel][pair of columns], padded against bank conflicts
-  const int64_t M = static_cast<int64_t>(g.B) * g.Hout * g.Wout;
-  const int k0 = blockIdx.x * 64;
-  const int64_t m0 = static_cast<int64_t>(blockIdx.y) * 64;
-  const int c8 = threadIdx.x & 7, pl = threadIdx.x >> 3;   // 8-column chunk, pixel within the tile (0..31)
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int p = pl + 32 * h;
-    const int64_t m = m0 + p;
-    const int k = k0 + 8 * c8;
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (m < M && k < K) {
-      const int64_t src = conv_src(g, m, k);
-      if (src >= 0) v = *reinterpret_cast<const uint4*>(x + src);
-      *reinterpret_cast<uint4*>(cols + m * K + k) = v;
-    }
-    tile[p][4 * c8 + 0] = v.x;
-    tile[p][4 * c8 + 1] = v.y;
-    tile[p][4 * c8 + 2] = v.z;
-    tile[p][4 * c8 + 3] = v.w;
-  }
-  __syncthreads();
-  // transposed: column index kk of the tile, pixels 2j and 2j+1 as one BF16 pair
-  const int j = threadIdx.x & 31, kr = threadIdx.x >> 5;
-  const int64_t m = m0 + 2 * j;
-#pragma unroll
-  for (int kk = kr; kk < 64; kk += 8) {
-    const int k = k0 + kk;
-    if (k >= K || m >= M) continue;
-    const uint32_t a = tile[2 * j][kk >> 1], b = tile[2 * j + 1][kk >> 1];
-    const uint16_t lo = (kk & 1) ? static_cast<uint16_t>(a >> 16) : static_cast<uint16_t>(a & 0xffffu);
-    const uint16_t hi = (kk & 1) ? static_cast<uint16_t>(b >> 16) : static_cast<uint16_t>(b & 0xffffu);
-    bf16* q = colst + static_cast<int64_t>(k) * ldt + m;
-    if (m + 1 < M) {
-      *reinterpret_cast<uint32_t*>(q) = static_cast<uint32_t>(lo) | (static_cast<uint32_t>(hi) << 16);
-    } else {
-      *reinterpret_cast<uint16_t*>(q) = lo;
-    }
-  }
-}
-
-// 4 channels per thread (Cin % 4 == 0 and a row stride Kc % 4 == 0): float4 gathers.
-__global__ void col2im_lrelu_vec4_kernel(const float* __restrict__ dcols, ConvGeom g, int Kc, const bf16* __restrict__ y,
-                                         float slope, bf16* __restrict__ dpre, int64_t ldp) {
-  const int chunks = g.Cin / 4;
-  const int64_t total = static_cast<int64_t>(g.B) * g.Hin * g.Win * chunks;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int c = static_cast<int>(i % chunks) * 4;
-    const int64_t pix = i / chunks;
-    const int ix = static_cast<int>(pix % g.Win);
-    const int64_t t = pix / g.Win;
-    const int iy = static_cast<int>(t % g.Hin);
-    const int b = static_cast<int>(t / g.Hin);
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int uy = iy * g.up; uy < (iy + 1) * g.up; ++uy)
-      for (int kh = 0; kh < g.KH; ++kh) {
-        const int ty = uy + g.ph - kh;
-        if (ty < 0 || ty % g.sh) continue;
-        const int oy = ty / g.sh;
-        if (oy >= g.Hout) continue;
-        for (int ux = ix * g.up; ux < (ix + 1) * g.up; ++ux)
-          for (int kw = 0; kw < g.KW; ++kw) {
-            const int tx = ux + g.pw - kw;
-            if (tx < 0 || tx % g.sw) continue;
-            const int ox = tx / g.sw;
-            if (ox >= g.Wout) continue;
-            const int64_t m = (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout + ox;
-            const float4 d = *reinterpret_cast<const float4*>(dcols + m * Kc + (kh * g.KW + kw) * g.Cin + c);
-            acc.x += d.x;
-            acc.y += d.y;
-            acc.z += d.z;
-            acc.w += d.w;
-          }
-      }
-    const float a[4] = {acc.x, acc.y, acc.z, acc.w};
-    bf16 o[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const float yv = __bfloat162float(y[pix * g.Cin + c + j]);
-      o[j] = __float2bfloat16_rn(yv > 0.f ? a[j] : slope * a[j]);
-    }
-    bf16* dst = dpre + pix * ldp + c;
-    if ((ldp & 3) == 0) {
-      *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(o);
-    } else {
-      for (int j = 0; j < 4; ++j) dst[j] = o[j];
-    }
-  }
-}
 
 // BF16 column gradients back onto the input, 8 channels per thread (16-byte
 // loads and stores), times the leaky-ReLU derivative of the layer below.
@@ -651,132 +539,6 @@ __global__ void __launch_bounds__(256) im2col_px_kernel(const bf16* __restrict__
       if (uy >= 0 && ux >= 0 && uy < Hup && ux < Wup)
         v = *reinterpret_cast<const uint4*>(xb + (static_cast<int64_t>(uy / UP) * g.Win + ux / UP) * g.Cin + c8 * 8);
       *reinterpret_cast<uint4*>(dst + j * 8) = v;
-    }
-  }
-}
-
-// Column gradients back onto the input (the transpose of im2col, as a
-// gather: no atomics, deterministic), times the leaky-ReLU derivative of the
-// layer below, whose output y is the input here: dpre = dx * (y > 0 ? 1 : slope).
-__global__ void col2im_lrelu_kernel(const float* __restrict__ dcols, ConvGeom g, int Kc, const bf16* __restrict__ y,
-                                    float slope, bf16* __restrict__ dpre, int64_t ldp) {
-  const int64_t total = static_cast<int64_t>(g.B) * g.Hin * g.Win * g.Cin;
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int c = static_cast<int>(i % g.Cin);
-    const int64_t pix = i / g.Cin;
-    const int ix = static_cast<int>(pix % g.Win);
-    const int64_t t = pix / g.Win;
-    const int iy = static_cast<int>(t % g.Hin);
-    const int b = static_cast<int>(t / g.Hin);
-    float acc = 0.f;
-    for (int uy = iy * g.up; uy < (iy + 1) * g.up; ++uy)
-      for (int kh = 0; kh < g.KH; ++kh) {
-        const int ty = uy + g.ph - kh;
-        if (ty < 0 || ty % g.sh) continue;
-        const int oy = ty / g.sh;
-        if (oy >= g.Hout) continue;
-        for (int ux = ix * g.up; ux < (ix + 1) * g.up; ++ux)
-          for (int kw = 0; kw < g.KW; ++kw) {
-            const int tx = ux + g.pw - kw;
-            if (tx < 0 || tx % g.sw) continue;
-            const int ox = tx / g.sw;
-            if (ox >= g.Wout) continue;
-            const int64_t m = (static_cast<int64_t>(b) * g.Hout + oy) * g.Wout + ox;
-            acc += dcols[m * Kc + (kh * g.KW + kw) * g.Cin + c];
-          }
-      }
-    const float yv = __bfloat162float(y[i]);
-    dpre[pix * ldp + c] = __float2bfloat16_rn(yv > 0.f ? acc : slope * acc);
-  }
-}
-
-__global__ void transpose_bf16_kernel(const bf16* __restrict__ in, int64_t ld_in, int R, int C, bf16* __restrict__ out,
-                                      int64_t ld_out) {
-  __shared__ bf16 tile[32][33];
-  const int64_t r0 = static_cast<int64_t>(blockIdx.y) * 32, c0 = static_cast<int64_t>(blockIdx.x) * 32;
-  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int64_t r = r0 + j, c = c0 + threadIdx.x;
-    if (r < R && c < C) tile[j][threadIdx.x] = in[r * ld_in + c];
-  }
-  __syncthreads();
-  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int64_t c = c0 + j, r = r0 + threadIdx.x;
-    if (r < R && c < C) out[c * ld_out + r] = tile[threadIdx.x][j];
-  }
-}
-
-// out[c][r] = in[r][c] for a [R][C] BF16 matrix (row strides ld_in, ld_out, both
-// even), in tiles of 64 rows x TW columns (TW = 64, or 32 for matrices of at
-// most 32 columns, so that narrow matrices keep every thread busy): rows are
-// read and written as BF16 pairs (4-byte accesses), staged in shared memory.
-// With colsum != NULL the CTA also adds the column sums of its rows into
-// colsum (float), one atomic per column per CTA: a CTA walks `tiles` row
-// tiles so that the atomics stay few.
-constexpr int kTT = 64;
-template <int TW>
-__global__ void __launch_bounds__(256) transpose_sum_kernel(const bf16* __restrict__ in, int64_t ld_in, int R, int C,
-                                                            bf16* __restrict__ out, int64_t ld_out,
-                                                            float* __restrict__ colsum, int tiles) {
-  constexpr int kPairs = TW / 2;              // threads per tile row when loading
-  constexpr int kRowsPass = 256 / kPairs;     // tile rows loaded per pass
-  __shared__ bf16 tile[kTT][TW + 2];
-  __shared__ float part[kRowsPass][TW];
-  const int tx = threadIdx.x % kPairs, ty = threadIdx.x / kPairs;
-  const int wx = threadIdx.x & 31, wy = threadIdx.x >> 5;   // store phase: 32 pairs of rows per column
-  const int c0 = blockIdx.x * TW;
-  const int c = c0 + 2 * tx;
-  float s0 = 0.f, s1 = 0.f;
-  for (int t = 0; t < tiles; ++t) {
-    const int64_t r0 = (static_cast<int64_t>(blockIdx.y) * tiles + t) * kTT;
-    if (r0 >= R) break;
-#pragma unroll
-    for (int j = ty; j < kTT; j += kRowsPass) {
-      const int64_t r = r0 + j;
-      bf16 a = __float2bfloat16(0.f), b = a;
-      if (r < R) {
-        const bf16* p = in + r * ld_in + c;
-        if (c + 1 < C) {
-          const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(p);
-          a = v.x;
-          b = v.y;
-        } else if (c < C) {
-          a = p[0];
-        }
-      }
-      tile[j][2 * tx] = a;
-      tile[j][2 * tx + 1] = b;
-      s0 += __bfloat162float(a);
-      s1 += __bfloat162float(b);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = wy; j < TW; j += 8) {
-      const int cc = c0 + j;
-      const int64_t r = r0 + 2 * wx;
-      if (cc < C && r < R) {
-        bf16* q = out + static_cast<int64_t>(cc) * ld_out + r;
-        if (r + 1 < R) {
-          __nv_bfloat162 v;
-          v.x = tile[2 * wx][j];
-          v.y = tile[2 * wx + 1][j];
-          *reinterpret_cast<__nv_bfloat162*>(q) = v;
-        } else {
-          q[0] = tile[2 * wx][j];
-        }
-      }
-    }
-    __syncthreads();
-  }
-  if (colsum) {
-    part[ty][2 * tx] = s0;
-    part[ty][2 * tx + 1] = s1;
-    __syncthreads();
-    if (threadIdx.x < TW && c0 + threadIdx.x < C) {
-      float s = 0.f;
-#pragma unroll
-      for (int k = 0; k < kRowsPass; ++k) s += part[k][threadIdx.x];
-      atomicAdd(colsum + c0 + threadIdx.x, s);
     }
   }
 }
@@ -1236,19 +998,15 @@ int32_t ss_gemm_bf16(const void* A, int64_t lda, const void* B, int64_t ldb, int
 }
 
 // conv: {B, Hin, Win, Cin, KH, KW, sh, sw, ph, pw, up}; the output size follows.
-int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t transposed, int64_t ldt, void* cols,
-                       void* stream) {
+int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, void* cols, void* stream) {
   ss_internal::clear_error();
   if (!x || !conv || !cols) return fail(SS_ERR_INVALID, "bad arguments");
   const ConvGeom g = conv_geom(conv);
   const int K = g.KH * g.KW * g.Cin;
   if (g.Hout < 1 || g.Wout < 1 || g.up < 1 || g.sh < 1 || g.sw < 1 || Kc < K) return fail(SS_ERR_INVALID, "bad convolution");
   const long long M = static_cast<long long>(g.B) * g.Hout * g.Wout;
-  if (transposed && ldt < M) return fail(SS_ERR_INVALID, "transposed columns need ldt >= pixels");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (transposed)
-    im2col_t_kernel<<<grid_for_l(M * K), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, ldt, static_cast<bf16*>(cols));
-  else if (g.Cin % 8 == 0 && Kc == K && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+  if (g.Cin % 8 == 0 && Kc == K && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
            (reinterpret_cast<uintptr_t>(cols) & 15) == 0 && (g.Cin & (g.Cin - 1)) == 0 && M * K / 8 < (1LL << 31) &&
            static_cast<long long>(g.B) * g.Hin * g.Win * g.Cin < (1LL << 31)) {
     int c8_shift = 0;
@@ -1278,45 +1036,6 @@ int32_t ss_im2col_bf16(const void* x, const int32_t* conv, int32_t Kc, int32_t t
                                                                              static_cast<bf16*>(cols));
   else
     im2col_kernel<<<grid_for_l(M * Kc), 256, 0, st>>>(static_cast<const bf16*>(x), g, K, Kc, static_cast<bf16*>(cols));
-  SS_TRY_CUDA(cudaGetLastError());
-  return SS_OK;
-}
-
-int32_t ss_im2col_both_bf16(const void* x, const int32_t* conv, int32_t Kc, void* cols, void* colst, int64_t ldt,
-                            void* stream) {
-  ss_internal::clear_error();
-  if (!x || !conv || !cols || !colst) return fail(SS_ERR_INVALID, "bad arguments");
-  const ConvGeom g = conv_geom(conv);
-  const int K = g.KH * g.KW * g.Cin;
-  if (g.Hout < 1 || g.Wout < 1 || g.up < 1 || g.sh < 1 || g.sw < 1) return fail(SS_ERR_INVALID, "bad convolution");
-  if (g.Cin % 8 != 0 || Kc != K || ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(cols)) & 15) != 0 ||
-      (reinterpret_cast<uintptr_t>(colst) & 3) != 0)
-    return fail(SS_ERR_UNSUPPORTED, "columns and transpose together need Cin % 8 == 0, Kc == K and aligned buffers");
-  const long long M = static_cast<long long>(g.B) * g.Hout * g.Wout;
-  if (ldt < M || (ldt & 1)) return fail(SS_ERR_INVALID, "transposed columns need an even ldt >= pixels");
-  const long long gy = (M + 63) / 64;
-  if (gy > 65535) return fail(SS_ERR_UNSUPPORTED, "too many pixels for one launch");
-  im2col_both_kernel<<<dim3((K + 63) / 64, static_cast<unsigned>(gy)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const bf16*>(x), g, K, ldt, static_cast<bf16*>(cols), static_cast<bf16*>(colst));
-  SS_TRY_CUDA(cudaGetLastError());
-  return SS_OK;
-}
-
-int32_t ss_col2im_lrelu_bf16(const float* dcols, const int32_t* conv, int32_t Kc, const void* y, float slope,
-                             void* dpre, int64_t ldp, void* stream) {
-  ss_internal::clear_error();
-  if (!dcols || !conv || !y || !dpre) return fail(SS_ERR_INVALID, "bad arguments");
-  const ConvGeom g = conv_geom(conv);
-  if (ldp < g.Cin) return fail(SS_ERR_INVALID, "ldp < channels");
-  const long long total = static_cast<long long>(g.B) * g.Hin * g.Win * g.Cin;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (g.Cin % 4 == 0 && Kc % 4 == 0 && (reinterpret_cast<uintptr_t>(dcols) & 15) == 0 &&
-      (reinterpret_cast<uintptr_t>(dpre) & 7) == 0)
-    col2im_lrelu_vec4_kernel<<<grid_for_l(total / 4), 256, 0, st>>>(dcols, g, Kc, static_cast<const bf16*>(y), slope,
-                                                                     static_cast<bf16*>(dpre), ldp);
-  else
-    col2im_lrelu_kernel<<<grid_for_l(total), 256, 0, st>>>(dcols, g, Kc, static_cast<const bf16*>(y), slope,
-                                                           static_cast<bf16*>(dpre), ldp);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
 }
@@ -1358,54 +1077,6 @@ int32_t ss_col2im16_lrelu_bf16(const void* dcols, const int32_t* conv, int32_t K
     col2im16_lrelu_kernel<0, 0, 0, 0, 0><<<grid, 256, 0, st>>>(dc, g, Kc, yy, slope, dp, ldp, n, c8_shift);
   SS_TRY_CUDA(cudaGetLastError());
   return SS_OK;
-}
-
-// Transpose (and optionally column sums) through the pair-wise kernel when
-// strides and addresses allow 4-byte BF16-pair accesses, else element-wise.
-static int transpose_launch(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, float* colsum,
-                     void* stream) {
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const bool pairs = (ld_in % 2 == 0) && (ld_out % 2 == 0) && (reinterpret_cast<uintptr_t>(in) % 4 == 0) &&
-                     (reinterpret_cast<uintptr_t>(out) % 4 == 0);
-  if (pairs) {
-    const int tw = C <= 32 ? 32 : 64;
-    const int gx = (C + tw - 1) / tw;
-    const long long row_tiles = (static_cast<long long>(R) + kTT - 1) / kTT;
-    // with column sums, enough row tiles per CTA that about 8 CTAs per SM remain (few atomics per column)
-    const int tiles = colsum ? static_cast<int>(std::max<long long>(1, row_tiles * gx / (148 * 8))) : 1;
-    const long long gy = (row_tiles + tiles - 1) / tiles;
-    if (gy > 65535) return fail(SS_ERR_UNSUPPORTED, "matrix too tall to transpose");
-    const dim3 grid(gx, static_cast<unsigned>(gy));
-    if (tw == 32)
-      transpose_sum_kernel<32><<<grid, 256, 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out),
-                                                     ld_out, colsum, tiles);
-    else
-      transpose_sum_kernel<64><<<grid, 256, 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C, static_cast<bf16*>(out),
-                                                     ld_out, colsum, tiles);
-  } else {
-    dim3 grid((C + 31) / 32, (R + 31) / 32);
-    transpose_bf16_kernel<<<grid, dim3(32, 8), 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C,
-                                                          static_cast<bf16*>(out), ld_out);
-    if (colsum) {
-      dim3 g2((C + 127) / 128, static_cast<unsigned>(std::min<long long>(R, 512)));
-      bias_grad_kernel<<<g2, 128, 0, st>>>(static_cast<const bf16*>(in), ld_in, R, C, colsum);
-    }
-  }
-  SS_TRY_CUDA(cudaGetLastError());
-  return SS_OK;
-}
-
-int32_t ss_transpose_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out, void* stream) {
-  ss_internal::clear_error();
-  if (!in || !out || R < 1 || C < 1 || ld_in < C || ld_out < R) return fail(SS_ERR_INVALID, "bad arguments");
-  return transpose_launch(in, ld_in, R, C, out, ld_out, nullptr, stream);
-}
-
-int32_t ss_transpose_sum_bf16(const void* in, int64_t ld_in, int32_t R, int32_t C, void* out, int64_t ld_out,
-                              float* colsum, void* stream) {
-  ss_internal::clear_error();
-  if (!in || !out || !colsum || R < 1 || C < 1 || ld_in < C || ld_out < R) return fail(SS_ERR_INVALID, "bad arguments");
-  return transpose_launch(in, ld_in, R, C, out, ld_out, colsum, stream);
 }
 
 int32_t ss_bias_grad_bf16(const void* dpre, int64_t ld, int64_t M, int32_t C, float* db, void* stream) {

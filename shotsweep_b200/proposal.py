@@ -217,7 +217,7 @@ class ProposalNet:
             hi, wi, ho, wo, K, Kc, N = self.shapes[i]
             M = self.B * (ho * wo if L.kind != 'fc' else 1)
             if L.kind == 'conv':
-                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, 0, 0, _lib.ptr(self.cols[i]),
+                _lib.check(self.L.ss_im2col_bf16(_lib.ptr(x), self._conv(i), Kc, _lib.ptr(self.cols[i]),
                                                  self._stream()), 'ss_im2col_bf16')
                 A, lda = self.cols[i], Kc
             else:

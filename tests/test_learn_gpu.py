@@ -224,7 +224,7 @@ def test_im2col_matches_unfold(conv):
     ref = _unfold_cols(x.float(), conv)
     cols = torch.full_like(ref, float('nan'), dtype=torch.bfloat16)
     L = _lib.load()
-    _lib.check(L.ss_im2col_bf16(_lib.ptr(x), (ctypes.c_int32 * 11)(*conv), ref.shape[1], 0, 0, _lib.ptr(cols),
+    _lib.check(L.ss_im2col_bf16(_lib.ptr(x), (ctypes.c_int32 * 11)(*conv), ref.shape[1], _lib.ptr(cols),
                                 _lib.stream_handle(x.device)), 'ss_im2col_bf16')
     torch.cuda.synchronize()
     assert torch.equal(cols.float(), ref)
