@@ -970,7 +970,10 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
   if (rc) return rc;
   rc = bmn ? make_tmap(&tb, B, N, K, ldb, 64) : make_tmap(&tb, B, K, N, ldb, bn);
   if (rc) return rc;
-  GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, std::min(kStagesG, per)};
+  // ring depth: no deeper than the CTA's K steps; two slots for split-K (weight-gradient) CTAs, so that three
+  // share an SM and more K slices stream at once (timed faster than one CTA with four slots)
+  const int stages = std::min(epi == SS_EPI_F32_ADD ? 2 : kStagesG, per);
+  GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, stages};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // BF16 outputs of one- or two-step K loops (epilogue-bound: the input-gradient GEMMs) leave through tile
   // stores where TMA can address their rows (16-byte aligned base and stride); with longer K loops the
