@@ -970,9 +970,12 @@ int32_t ss_gemm_bf16_layout(const void* A, int64_t lda, const void* B, int64_t l
   if (rc) return rc;
   rc = bmn ? make_tmap(&tb, B, N, K, ldb, 64) : make_tmap(&tb, B, K, N, ldb, bn);
   if (rc) return rc;
-  // ring depth: no deeper than the CTA's K steps; two slots for split-K (weight-gradient) CTAs, so that three
-  // share an SM and more K slices stream at once (timed faster than one CTA with four slots)
-  const int stages = std::min(epi == SS_EPI_F32_ADD ? 2 : kStagesG, per);
+  // ring depth: no deeper than the CTA's K steps, and the deepest ring with which two CTAs share an SM
+  // (4 slots for tiles up to 64 wide, 3 for 128, 2 for 256: one CTA's epilogue then overlaps the other's
+  // loads and MMAs); two slots for split-K (weight-gradient) CTAs, so that three share an SM.  Each choice
+  // timed faster than one CTA per SM with four slots.
+  const int fit2 = bn >= 256 ? 2 : bn >= 128 ? 3 : kStagesG;
+  const int stages = std::min(epi == SS_EPI_F32_ADD ? 2 : fit2, per);
   GemmArgs g{M, N, K, k_tiles, per, C, ldc, bias, slope, err, stages};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // BF16 outputs of one- or two-step K loops (epilogue-bound: the input-gradient GEMMs) leave through tile
