@@ -55,8 +55,6 @@ constexpr int kDefaultRows = 5;
 __host__ __device__ constexpr int max_threads_for(int H) { return H <= 3 ? 640 : H == 4 ? 512 : H == 5 ? 384 : 320; }
 constexpr int kMinRows = 3, kMaxRows = 6;
 constexpr int kMaxCluster = 16;
-constexpr int kTraceRing = 32;             // receiver rows staged in shared memory per flush (at most)
-constexpr int kMinTraceRing = 8;           // the fewest, for grids whose shared memory is tight
 // Adjoint history slabs in shared memory (prefetch depth: slabs - 1): four on
 // the OpenFWI fast path (timed 0.7 % faster than three), three for every other
 // grid and for uneven batches, whose large grids need the shared memory for
@@ -223,7 +221,6 @@ struct KParams {
   float dx, dt;
   int ncg, nseg, bh, C, rs, sw, nact;
   int nxs;         // trace row stride of the per-slot scratch (nx rounded up to 4)
-  int ring;        // receiver rows staged in shared memory per flush (a power of two, 8..32)
   int n_solves;
   const float* vel;
   const float* wav;
@@ -264,7 +261,6 @@ struct Smem {
   float* wav;
   float* red;
   float* res0;     // kStages residual rows of nxs, consecutive
-  float* trc;      // ring of P.ring receiver rows, flushed to global memory
   float* dummy;    // zero tile for lanes without cells: (H + 4) rows of RS, then H rows of sw
   uint64_t* bar;
 };
@@ -552,8 +548,7 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
     S.wav = base + 2 * field_floats + kStages * stage_floats;
     S.red = S.wav + ((P.nt + 31) & ~31);
     S.res0 = S.red + 32;
-    S.trc = S.res0 + kStages * NXS;
-    S.dummy = S.trc + P.ring * NXS;
+    S.dummy = S.res0 + kStages * NXS;
     S.bar = reinterpret_cast<uint64_t*>(S.dummy + (H + 4) * RS + H * SW);   // [0,kStages) history, then 2 halos
     {   // self-check: the layout (barriers and the TMEM address word last) must fit the launch's allocation;
         // every CTA of the cluster computes the same sizes, so all of them return together
@@ -571,8 +566,7 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
     S.wav = reinterpret_cast<float*>(smem_raw) + 16;   // 64-byte aligned after the barriers
     S.red = S.wav + ((P.nt + 31) & ~31);
     S.res0 = S.red + 32;
-    S.trc = S.res0 + kStages * NXS;
-    solve_smem = S.trc + P.ring * NXS;
+    solve_smem = S.res0 + kStages * NXS;
   }
   for (int i = tid; i < P.nt; i += nthr) S.wav[i] = P.wav[i];
   if (tid == 0) {
@@ -773,7 +767,6 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
 
     const int tstride = (MODE == SS_MODE_FORWARD) ? NX : NXS;
     float src_acc = 0.f;   // sum_t th(source cell) * w[t]
-    int flushed = 0;       // receiver rows below this level are in global memory
     float* trace = (MODE == SS_MODE_FORWARD) ? P.gathers + trc_off : P.trace + static_cast<size_t>(slot) * trace_slot;
 
     // ---- this model's wavelet (one per model: forward and gradient modes),
@@ -845,10 +838,12 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
       const bool push_up = more && edge_up, push_dn = more && edge_dn;
       if (!SEG && fwd && rank == rec_rank && step > 0 && warp_recv) {
         // receivers at every model column (gpu.py:134): the level recorded at
-        // the previous step is now the read-only field X
+        // the previous step is now the read-only field X; one coalesced row
+        // straight to global memory per step (a shared ring flushed in bursts
+        // held up this CTA, which paces the cluster, every ring-full of steps)
         #pragma unroll 1
         for (int r = tid; r < NX; r += nthr)
-          S.trc[((lvl - 1) & (P.ring - 1)) * NXS + r] = X[(src_r - row0 + 2) * RS + PAD + r + 2];
+          trace[static_cast<size_t>(lvl - 1) * tstride + r] = X[(src_r - row0 + 2) * RS + PAD + r + 2];
       }
       {
         // Lanes without a tile run the same code on a private zero tile
@@ -929,28 +924,13 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
         }
       }
       __syncthreads();
-      if (!SEG && fwd && rank == rec_rank) {
-        // The ring holds the receiver rows [flushed, lvl-1] (level lvl-1 was
-        // recorded at this step's start).  A full ring, and at the end every
-        // remaining row, goes to global memory, coalesced.
-        auto flush = [&](int hi) {
-          __syncthreads();
-          const int n = (hi - flushed + 1) * NX;
-          #pragma unroll 1
-          for (int i = tid; i < n; i += nthr) {
-            const int tt = flushed + i / NX, r = i % NX;
-            trace[static_cast<size_t>(tt) * tstride + r] = S.trc[(tt & (P.ring - 1)) * NXS + r];
-          }
-          __syncthreads();
-          flushed = hi + 1;
-        };
-        if (lvl - flushed == P.ring) flush(lvl - 1);
-        if (lvl == GNT - 1) {   // the last level, recorded after the final barrier
-          #pragma unroll 1
+      if (!SEG && fwd && rank == rec_rank && lvl == GNT - 1) {
+        // the last level, recorded after the final barrier; the barrier after
+        // it publishes every recorded row to the CTA's residual pass
+        #pragma unroll 1
         for (int r = tid; r < NX; r += nthr)
-            S.trc[(lvl & (P.ring - 1)) * NXS + r] = Y[(src_r - row0 + 2) * RS + PAD + r + 2];
-          flush(lvl);
-        }
+          trace[static_cast<size_t>(lvl) * tstride + r] = Y[(src_r - row0 + 2) * RS + PAD + r + 2];
+        __syncthreads();
       }
     };
 
@@ -1333,7 +1313,7 @@ __global__ void __launch_bounds__(256) fp32_probe_kernel(float* out, int iters) 
 // Host side: plans, workspace, launches
 // ----------------------------------------------------------------------------
 struct Plan {
-  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads, ring, H;
+  int nzp, nxp, ncg, nseg, bh, C, rs, sw, threads, H;
   bool fast;
   size_t smem;
   int max_clusters;
@@ -1401,12 +1381,12 @@ int rows_for_mode(int mode) {
   return fixed_rows_ok(r) ? r : kDefaultRows;
 }
 
-size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int ring, int H, bool fast) {
+size_t smem_bytes(int bh, int rs, int sw, int nt, int nxs, bool adj, int H, bool fast) {
   const int slabs = fast ? kStagesFast : kStagesGeneric;   // what solve_kernel<.., fast, false, ..> lays out
   const size_t field = static_cast<size_t>(bh + 4) * rs;
   const size_t stage = adj ? static_cast<size_t>(bh) * sw : 0;
   return (2 * field + slabs * stage + ((nt + 31) & ~31) + 32 +
-          (slabs + ring) * static_cast<size_t>(nxs) + (H + 4) * static_cast<size_t>(rs) +
+          slabs * static_cast<size_t>(nxs) + (H + 4) * static_cast<size_t>(rs) +
           H * static_cast<size_t>(sw)) *
              sizeof(float) +
          (slabs + 3) * sizeof(uint64_t);   // barriers, then the TMEM address word
@@ -1432,20 +1412,15 @@ int plan_shape(const ss_geometry* g, int mode, Plan* p) {
     if (C > 1 && nseg < 1) break;
     const int bh = nseg * H;
     if (C > 1 && bh < 2) continue;
-    // the deepest receiver ring that fits (wide grids with long time axes get a shallower one)
-    for (int ring = kTraceRing; ring >= kMinTraceRing && !ok; ring /= 2) {
-      const size_t sm =
-          smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj, ring, H, fast_geometry(g->nx, g->pad));
-      if (sm <= kMaxSmem) {
-        p->C = C;
-        p->nseg = nseg;
-        p->bh = bh;
-        p->smem = sm;
-        p->ring = ring;
-        ok = true;
-      }
+    const size_t sm = smem_bytes(bh, p->rs, p->sw, g->nt, (g->nx + 3) & ~3, adj, H, fast_geometry(g->nx, g->pad));
+    if (sm <= kMaxSmem) {
+      p->C = C;
+      p->nseg = nseg;
+      p->bh = bh;
+      p->smem = sm;
+      ok = true;
+      break;
     }
-    if (ok) break;
   }
   if (!ok) return fail(SS_ERR_UNSUPPORTED, "no cluster plan fits shared memory for this grid");
   p->threads = ((p->ncg * p->nseg + 31) / 32) * 32;
@@ -1557,7 +1532,6 @@ KParams base_params(const ss_geometry* g, const Plan& p, int n_models) {
   k.sw = p.sw;
   k.nact = p.ncg * p.nseg;
   k.nxs = (g->nx + 3) & ~3;
-  k.ring = p.ring > 0 ? p.ring : kTraceRing;
   k.n_solves = n_models * g->n_shots;
   k.hist_steps = g->nt;
   return k;
@@ -1668,11 +1642,11 @@ int noalloc_scratch(void** out) {
 // A plan is one contiguous blob, identical in host and device memory:
 // BatchPlanHeader, then BatchItemDev[n_items], then int order[n_solves]
 // (per class, solves longest-first).  The header carries the launch shapes.
-constexpr uint64_t kPlanMagic = 0x3330504853535342ull;   // "BSSSHP03"
+constexpr uint64_t kPlanMagic = 0x3430504853535342ull;   // "BSSSHP04"
 constexpr int kMaxClasses = 32;   // (cluster size, tile height) pairs of one plan
 
 struct BatchClassHost {
-  int C, H, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter, ring;
+  int C, H, min_C, threads, slots, smem, stream, n_solves, order_begin, nt_max, nxs, bh_max, counter;
   int max_clusters, idle_sms;   // co-resident clusters alone on the GPU, and the SMs they leave idle
   size_t hist_slot, trace_slot, gpad_slot, grad_slot;   // floats per slot
   size_t ws_off;                                        // bytes: this class's scratch in the workspace
@@ -1688,10 +1662,10 @@ struct BatchPlanHeader {
 };
 
 // Shared memory of a batch launch: the fixed part (barriers, wavelet,
-// reduction words, residual rows, receiver ring) and one solve's part
+// reduction words, residual rows) and one solve's part
 // (two fields, the history slabs, the zero tile).
-size_t batch_fixed_smem(int nt_max, int nxs, int ring = kMinTraceRing) {
-  return (16 + static_cast<size_t>((nt_max + 31) & ~31) + 32 + static_cast<size_t>(kStagesGeneric + ring) * nxs) *
+size_t batch_fixed_smem(int nt_max, int nxs) {
+  return (16 + static_cast<size_t>((nt_max + 31) & ~31) + 32 + static_cast<size_t>(kStagesGeneric) * nxs) *
          sizeof(float);
 }
 size_t batch_solve_smem(int bh, int ncg, bool adj, int H) {
@@ -1919,13 +1893,7 @@ int batch_plan(const ss_physics* phys, int mode, const ss_batch_item* items, int
     }
     k.trace_slot = static_cast<size_t>(k.nt_max) * k.nxs;
     k.threads = ((max_nact + 31) / 32) * 32;
-    k.ring = kMinTraceRing;   // the deepest receiver ring that fits beside the class's largest solve
-    for (int ring = kTraceRing; ring > kMinTraceRing; ring /= 2)
-      if (batch_fixed_smem(k.nt_max, k.nxs, ring) + solve_part <= kMaxSmem) {
-        k.ring = ring;
-        break;
-      }
-    k.smem = static_cast<int>(batch_fixed_smem(k.nt_max, k.nxs, k.ring) + solve_part);
+    k.smem = static_cast<int>(batch_fixed_smem(k.nt_max, k.nxs) + solve_part);
     // solves longest-first
     const int begin = static_cast<int>(order.size());
     for (int i : cls[c].items)
@@ -2081,7 +2049,6 @@ int batch_run(const void* plan, const void* plan_dev, const float* vel, const fl
     p.C = k.C;
     p.nt = k.nt_max;
     p.nxs = k.nxs;
-    p.ring = k.ring;
     p.bh = k.bh_max;
     p.n_solves = k.n_solves;
     p.items = reinterpret_cast<const BatchItemDev*>(pd + h.items_off);
