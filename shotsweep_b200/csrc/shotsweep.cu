@@ -271,6 +271,10 @@ __device__ __forceinline__ float mute_weight(int t, int r, int shot_col, float d
   const float tt = static_cast<float>(t) * dt;
   const float t0 = h / vm + t_mute;
   const float ramp = fminf(fmaxf((tt - t0) / 0.03f, 0.f), 1.f);
+  // before and after the ramp the weight is exactly 0 and 1 (as the reference's float64 value); the cosine
+  // is needed only inside it
+  if (ramp <= 0.f) return 0.f;
+  if (ramp >= 1.f) return 1.f;
   return 0.5f - 0.5f * cosf(3.14159265358979323846f * ramp);
 }
 
@@ -1000,6 +1004,8 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
         acc[k][0] = acc[k][1] = A[k][0] = A[k][1] = B[k][0] = B[k][1] = make_float2(0.f, 0.f);
     }
     // ---- residual (sim - obs) * mute, in place over the trace ------------
+    // the receiver CTA's recorded rows, visible to every CTA of the cluster
+    cluster_sync();
     if (SEG && rank == rec_rank) {   // segment mode: the adjoint source is given
       const float* rg = P.res_in + static_cast<size_t>(solve) * P.nt * NX;
 #pragma unroll 1
@@ -1009,10 +1015,17 @@ __global__ void __launch_bounds__(max_threads_for(H), 1) solve_kernel(const KPar
       }
       fence_proxy_async_all();
       __syncthreads();
-    } else if (rank == rec_rank) {
+    } else if (!SEG) {
+      // every CTA of the cluster takes a contiguous share of the receiver CTA's
+      // trace (one CTA alone kept the others waiting at the next cluster
+      // barrier); the fence and that barrier publish the rows to the receiver
+      // CTA's bulk copies.  (Segment mode has no observations: its adjoint
+      // source comes in res_in and only the receiver CTA copies it, above.)
       const float* ob = P.obs + trc_off;
       const float vm = v_mute;
-      for (int i = tid; i < GNT * NX; i += nthr) {
+      const int total = GNT * NX, share = (total + P.C - 1) / P.C;
+      const int i1 = min(total, (rank + 1) * share);
+      for (int i = rank * share + tid; i < i1; i += nthr) {
         const int t = i / NX, r = i - t * NX;
         const float o = ob[i];
         if (!isfinite(o)) atomicExch(P.err, static_cast<int>(SS_ERR_NONFINITE));
